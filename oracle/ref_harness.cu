@@ -1,0 +1,149 @@
+/*
+ * ref_harness.cu -- runs the REFERENCE's own cost functors on the host (TEST
+ * INFRASTRUCTURE: parity oracle and timed CPU baseline; never part of the product).
+ *
+ * This file contains no reference code.  It #includes the unmodified reference headers
+ * from the reference checkout at build time (oracle/Makefile, REF=...), instantiates the
+ * __host__ __device__ functors (cudaErrorFunctions.cuh, cudaErrorFunction_mi.cuh) and
+ * calls them with CudaImage objects whose _data are host pointers, exactly as the
+ * reference itself does for its "Min Value check" (src/gpu/cudaGridSearch_main_mi.cu:388)
+ * and its Levenberg-Marquardt functor (src/cpu/multispectral_ImageMatcher.cu:283-298).
+ * The output, oracle/_ref/libcgs_ref.so, is not committed.
+ *
+ * The reference only decodes grid points on the device (CudaGrid::indexToGridPoint,
+ * cudaGridSearch.cuh:160-187); the harness decodes with the same integer arithmetic and
+ * takes the grid-value rounding mode (fused or not) as an argument.
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <omp.h>
+
+#define CUDAFUNCTION __host__ __device__
+#include "helper_cuda.h"
+#include <cudaTensor.cuh>
+#include "cudaGridSearch.cuh"
+#include "cudaErrorFunctions.cuh"
+#include "cudaErrorFunction_mi.cuh"
+
+namespace {
+
+enum { SAD_AVG = 0, SAD_AVG_H = 1, SAD_SUM_T = 2, SAD_SUM_T_REF = 3, SQD_REF = 4, NCC_REF = 5,
+       SQD_ALT = 6, NCC_ALT = 7, MI_ALT = 8 };
+
+// Images are passed padded: the caller allocates (H + 1) * W * C + C elements with zeros
+// after the image so the reference's reads at ceil(y) == H stay inside the buffer.
+template <typename P, uint32_t C>
+float eval_c(int cost, const float *params, const void *mov, int mh, int mw, const void *fix, int fh, int fw) {
+    CudaImage<P, C> M(mh, mw), F(fh, fw);
+    M.data() = (P *)mov;
+    F.data() = (P *)fix;
+    nv_ext::Vec<float, 8> v(params);
+    switch (cost) {
+        case SAD_AVG: return averageAbsoluteDifference<float, float, 8, C, P>(v, M, F);
+        case SQD_REF: return calcSQD<float, float, 8, C, P>(v, M, F);
+        case NCC_REF: return calcNCC<float, float, 8, C, P>(v, M, F);
+        case SQD_ALT: return calcSQDAlt<float, float, 8, C, P>(v, M, F);
+        case NCC_ALT: return calcNCCAlt<float, float, 8, C, P>(v, M, F);
+        case MI_ALT: return calcMIAlt<float, float, 8, C, P>(v, M, F);
+        default: break;
+    }
+    if (C == 1) {
+        CudaImage<P> M1(mh, mw), F1(fh, fw);
+        M1.data() = (P *)mov;
+        F1.data() = (P *)fix;
+        switch (cost) {
+            case SAD_AVG_H: return averageAbsoluteDifferenceH<float, float, 8, 1, P>(v, M1, F1);
+            case SAD_SUM_T: return sumOfAbsoluteDifferences<float, float, 8, 1, P>(v, M1, F1);
+            case SAD_SUM_T_REF: return sumOfAbsoluteDifferences<float, float, 8, 1, P>(v, &M1, &F1);
+            default: break;
+        }
+    }
+    return NAN;
+}
+
+template <typename P>
+float eval_p(int cost, const float *params, const void *mov, int mh, int mw, const void *fix, int fh, int fw, int c) {
+    switch (c) {
+        case 1: return eval_c<P, 1>(cost, params, mov, mh, mw, fix, fh, fw);
+        case 3: return eval_c<P, 3>(cost, params, mov, mh, mw, fix, fh, fw);
+        default: return NAN;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+/* One reference functor evaluation. pix: 0 = float, 1 = uint8_t. */
+float cgsref_eval(int cost, const float *params, int pix, const void *mov, int mh, int mw, const void *fix, int fh,
+                  int fw, int channels) {
+    if (pix == 1) return eval_p<uint8_t>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+    return eval_p<float>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+}
+
+/* The reference's homography helpers, for bit-exact tests of the oracle restatement. */
+void cgsref_params_to_h(const float *params, float cx, float cy, float *h) {
+    nv_ext::Vec<float, 8> v(params);
+    parametersToHomography<float, 8>(v, cx, cy, h[0], h[1], h[2], h[3], h[4], h[5], h[6], h[7]);
+}
+
+void cgsref_params_to_h_norm(const float *params, int mw, int mh, int fw, int fh, float *h) {
+    nv_ext::Vec<float, 8> v(params);
+    parametersToHomographyNorm<float, 8>(v, mw, mh, fw, fh, h[0], h[1], h[2], h[3], h[4], h[5], h[6], h[7]);
+}
+
+void cgsref_new_coord(const float *h_in, int x, int y, float *nx, float *ny) {
+    float h[8];
+    memcpy(h, h_in, sizeof(h));
+    calcNewCoordH(h[0], h[1], h[2], h[3], h[4], h[5], h[6], h[7], x, y, *nx, *ny);
+}
+
+float cgsref_bilinear(int pix, const void *data, int height, int width, float y, float x) {
+    if (pix == 1) {
+        CudaImage<uint8_t, 1> im(height, width);
+        im.data() = (uint8_t *)data;
+        return im.valueAt_bilinear(y, x, 0);
+    }
+    CudaImage<float, 1> im(height, width);
+    im.data() = (float *)data;
+    return im.valueAt_bilinear(y, x, 0);
+}
+
+/* Grid decode with the reference's integer arithmetic (cudaGridSearch.cuh:160-187).
+ * counts/start/res as stored in the CudaGrid matrix after update(). */
+static void decode(int dims, const float *start, const float *res, const float *count, int64_t index, int use_fma,
+                   float *out) {
+    int32_t inc[8], idx[8];
+    inc[0] = 1;
+    for (int a = 1; a < dims; a++) inc[a] = (int32_t)(count[a - 1] * (float)inc[a - 1]);
+    int32_t rem = (int32_t)index;
+    for (int a = dims - 1; a >= 0; a--) {
+        idx[a] = rem / inc[a];
+        rem -= idx[a] * inc[a];
+    }
+    for (int a = 0; a < 8; a++) out[a] = 0.0f;
+    for (int a = 0; a < dims; a++)
+        out[a] = use_fma ? fmaf((float)idx[a], res[a], start[a]) : start[a] + (float)idx[a] * res[a];
+}
+
+/* Reference functor over a strided sample of grid indices, OpenMP over all requested
+ * threads (the timed CPU baseline).  costs[k] = cost at index first + k * stride. */
+int cgsref_search(int cost, int dims, const float *start, const float *res, const float *count, int use_fma, int pix,
+                  const void *mov, int mh, int mw, const void *fix, int fh, int fw, int channels, int64_t first,
+                  int64_t n, int64_t stride, float *costs, int threads) {
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
+    for (int64_t k = 0; k < n; k++) {
+        float pt[8];
+        decode(dims, start, res, count, first + k * stride, use_fma, pt);
+        costs[k] = cgsref_eval(cost, pt, pix, mov, mh, mw, fix, fh, fw, channels);
+    }
+    return 0;
+}
+
+int cgsref_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"
