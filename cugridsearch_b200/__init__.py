@@ -1,0 +1,282 @@
+"""cugridsearch_b200 -- B200 (sm_100a) homography grid search behind the cuGridSearch API.
+
+The compute runs in ``libcgs_b200.so`` (hand-written CUDA for sm_100a, C ABI in
+``include/cugridsearch_b200.h``).  This module is the Python host mirror of the
+reference's template API (``src/gpu/cudaGridSearch.cuh``, ``include/cudaTensor.cuh``):
+
+=========================================  ===============================================
+reference                                  here
+=========================================  ===============================================
+``CudaGrid<float, D>`` + setters           :class:`CudaGrid`
+``CudaImage<T, C>`` (caller-owned data)     :class:`CudaImage` (wraps a CUDA tensor)
+``CudaTensor<float, D>`` result + find_extrema  :class:`CudaTensor`
+``CudaGridSearcher<F, G, D>::search*``      :class:`CudaGridSearcher`
+device functor pointer (``calcNCC`` ...)    cost names: :data:`calcNCC` etc.
+=========================================  ===============================================
+
+Device memory and streams come from PyTorch tensors; nothing here computes a cost.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import COSTS, CgsArgmin, CgsError, CgsGrid, CgsImage, CgsOptions, check
+
+__all__ = [
+    "CudaGrid", "CudaImage", "CudaTensor", "CudaGridSearcher", "Argmin", "search", "argmin",
+    "COSTS", "CgsError", "library", "averageAbsoluteDifference", "averageAbsoluteDifferenceH",
+    "sumOfAbsoluteDifferences", "sumOfAbsoluteDifferences_by_reference", "calcSQD", "calcNCC",
+    "calcSQDAlt", "calcNCCAlt", "calcMIAlt", "ZNCC", "MI",
+]
+
+# Cost selectors named after the reference functors (the device function pointer the
+# reference passes to search_by_value).
+averageAbsoluteDifference = "SAD_AVG"          # cudaErrorFunctions.cuh:31-87
+averageAbsoluteDifferenceH = "SAD_AVG_H"       # cudaErrorFunctions.cuh:194-224
+sumOfAbsoluteDifferences = "SAD_SUM_T"         # cudaErrorFunctions.cuh:89-114 (by value)
+sumOfAbsoluteDifferences_by_reference = "SAD_SUM_T_REF"  # cudaErrorFunctions.cuh:171-192
+calcSQD = "SQD_REF"                            # cudaErrorFunctions.cuh:378-446
+calcNCC = "NCC_REF"                            # cudaErrorFunctions.cuh:448-507
+calcSQDAlt = "SQD_ALT"                         # cudaErrorFunctions.cuh:226-300
+calcNCCAlt = "NCC_ALT"                         # cudaErrorFunctions.cuh:302-376
+calcMIAlt = "MI_ALT"                           # cudaErrorFunction_mi.cuh:117-255
+ZNCC = "ZNCC"
+MI = "MI"
+
+
+def library() -> C.CDLL:
+    return _abi.load()
+
+
+def _torch():
+    import torch  # device memory and streams only
+    return torch
+
+
+def _stream_handle(stream) -> int:
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream)
+
+
+@dataclass
+class Argmin:
+    cost: float
+    index: int
+    params: np.ndarray
+    valid: bool
+    status: int = 0
+
+    @staticmethod
+    def from_struct(r: CgsArgmin) -> "Argmin":
+        return Argmin(float(r.cost), int(r.index), np.array(list(r.params), dtype=np.float32), bool(r.valid),
+                      int(r.status))
+
+
+class CudaGrid:
+    """CudaGrid<float, D> (src/gpu/cudaGridSearch.cuh:74-231): rows {start, end,
+    resolution, count}; every setter calls update() as the reference's do (:198-215)."""
+
+    def __init__(self, dims: int = 8):
+        if not 1 <= dims <= 8:
+            raise ValueError("dims must be 1..8")
+        self.g = CgsGrid()
+        self.g.dims = dims
+        for a in range(8):
+            self.g.count[a] = 1.0
+
+    @classmethod
+    def from_ranges(cls, start, end, count) -> "CudaGrid":
+        g = cls(len(start))
+        g.setStartPoint(start)
+        g.setEndPoint(end)
+        g.setNumSamples(count)
+        return g
+
+    def getDimension(self) -> int:
+        return int(self.g.dims)
+
+    def _set_row(self, row, vals):
+        if len(vals) != self.g.dims:
+            raise ValueError(f"expected {self.g.dims} values")
+        for a, v in enumerate(vals):
+            row[a] = float(np.float32(v))
+        self.update()
+
+    def setStartPoint(self, vals):
+        self._set_row(self.g.start, vals)
+
+    def setEndPoint(self, vals):
+        self._set_row(self.g.end, vals)
+
+    def setNumSamples(self, vals):
+        self._set_row(self.g.count, vals)
+
+    def update(self, changed_axis: int = -1):
+        check(_abi.load().cgs_grid_update(C.byref(self.g), changed_axis))
+
+    def getAxisSampleCounts(self) -> np.ndarray:
+        return np.array(list(self.g.count)[: self.g.dims], dtype=np.float32)
+
+    def resolution(self) -> np.ndarray:
+        return np.array(list(self.g.resolution)[: self.g.dims], dtype=np.float32)
+
+    def numElements(self) -> int:
+        n = C.c_uint64(0)
+        check(_abi.load().cgs_grid_num_elements(C.byref(self.g), C.byref(n)))
+        return int(n.value)
+
+    def getGridPoint(self, index: int) -> np.ndarray:
+        out = (C.c_float * 8)()
+        check(_abi.load().cgs_grid_point(C.byref(self.g), int(index), out))
+        return np.array(list(out)[: self.g.dims], dtype=np.float32)
+
+    def matrix(self) -> np.ndarray:
+        """The 4 x D device matrix layout of the reference (rows start/end/res/count)."""
+        d = self.g.dims
+        return np.array([list(self.g.start)[:d], list(self.g.end)[:d], list(self.g.resolution)[:d],
+                         list(self.g.count)[:d]], dtype=np.float32)
+
+
+class CudaImage:
+    """CudaImage<T, C> (include/cudaTensor.cuh:507-596) over a caller-owned CUDA tensor of
+    shape (H, W) or (H, W, C), dtype float32 or uint8, HWC row-major."""
+
+    def __init__(self, tensor):
+        torch = _torch()
+        if not isinstance(tensor, torch.Tensor) or not tensor.is_cuda:
+            raise TypeError("CudaImage wraps a CUDA tensor (device memory is caller-owned)")
+        if tensor.dim() == 2:
+            tensor = tensor.unsqueeze(-1)
+        if tensor.dim() != 3 or not tensor.is_contiguous():
+            raise ValueError("expected a contiguous (H, W) or (H, W, C) tensor")
+        if tensor.dtype == torch.float32:
+            pix = _abi.PIXEL_F32
+        elif tensor.dtype == torch.uint8:
+            pix = _abi.PIXEL_U8
+        else:
+            raise TypeError("pixel type must be float32 or uint8")
+        self.tensor = tensor
+        h, w, c = tensor.shape
+        self.img = CgsImage(tensor.data_ptr(), h, w, c, pix)
+
+    def height(self) -> int:
+        return int(self.img.height)
+
+    def width(self) -> int:
+        return int(self.img.width)
+
+    def channels(self) -> int:
+        return int(self.img.channels)
+
+
+class CudaTensor:
+    """CudaTensor<float, D> result tensor (include/cudaTensor.cuh:108-361) on a CUDA tensor."""
+
+    def __init__(self, tensor):
+        torch = _torch()
+        if tensor.dtype != torch.float32 or not tensor.is_cuda or not tensor.is_contiguous():
+            raise TypeError("expected a contiguous float32 CUDA tensor")
+        self.tensor = tensor
+
+    def size(self) -> int:
+        return int(self.tensor.numel())
+
+    def find_extrema(self, stream=None) -> tuple[float, int]:
+        """find_extrema (include/cudaTensor.cuh:215-265): (min value, flat index)."""
+        torch = _torch()
+        out = torch.empty(C.sizeof(CgsArgmin), dtype=torch.uint8, device=self.tensor.device)
+        s = _stream_handle(stream)
+        check(_abi.load().cgs_argmin_f32(self.tensor.data_ptr(), self.tensor.numel(), out.data_ptr(), s))
+        host = out.cpu().numpy().tobytes()
+        r = CgsArgmin.from_buffer_copy(host)
+        return float(r.cost), int(r.index)
+
+
+def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0,
+             warps_per_block: int = 0, natural_order: bool = False) -> CgsOptions:
+    if cost not in COSTS:
+        raise ValueError(f"unknown cost {cost!r}")
+    return CgsOptions(COSTS[cost], mi_bins, overlap_gate, points_per_warp, warps_per_block,
+                      _abi.FLAG_NATURAL_ORDER if natural_order else 0)
+
+
+def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs=None, stream=None,
+           mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0, warps_per_block: int = 0,
+           natural_order: bool = False, result=None) -> Argmin | None:
+    """Run one fused search.  With ``result`` (a CUDA uint8 tensor of sizeof(cgs_argmin)
+    bytes) the call is asynchronous and returns None; otherwise it synchronises and
+    returns the :class:`Argmin`."""
+    opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order)
+    cptr = costs.data_ptr() if costs is not None else None
+    s = _stream_handle(stream)
+    L = _abi.load()
+    if result is not None:
+        check(L.cgs_search(C.byref(moving.img), C.byref(fixed.img), C.byref(grid.g), C.byref(opt), cptr,
+                           result.data_ptr(), s))
+        return None
+    r = CgsArgmin()
+    check(L.cgs_search_sync(C.byref(moving.img), C.byref(fixed.img), C.byref(grid.g), C.byref(opt), cptr,
+                            C.byref(r), s))
+    return Argmin.from_struct(r)
+
+
+def argmin(values, stream=None) -> Argmin:
+    torch = _torch()
+    out = torch.empty(C.sizeof(CgsArgmin), dtype=torch.uint8, device=values.device)
+    check(_abi.load().cgs_argmin_f32(values.data_ptr(), values.numel(), out.data_ptr(), _stream_handle(stream)))
+    return Argmin.from_struct(CgsArgmin.from_buffer_copy(out.cpu().numpy().tobytes()))
+
+
+def result_buffer(device=None):
+    """A device buffer for one asynchronous cgs_argmin result."""
+    torch = _torch()
+    return torch.empty(C.sizeof(CgsArgmin), dtype=torch.uint8, device=device or "cuda")
+
+
+def read_result(buf) -> Argmin:
+    return Argmin.from_struct(CgsArgmin.from_buffer_copy(buf.cpu().numpy().tobytes()))
+
+
+class CudaGridSearcher:
+    """CudaGridSearcher<float, float, D> (src/gpu/cudaGridSearch.cuh:540-855).
+
+    Every search variant evaluates the same function of each grid point, so all of them
+    run the one fused kernel; the launch-shape arguments of the stream/block variants
+    (STREAM_BLOCK_DIM, numCores, numThreads) are accepted and ignored.  The result tensor
+    receives the per-point costs, as the reference's does."""
+
+    def __init__(self, grid: CudaGrid, result: CudaTensor | None):
+        self._grid = grid
+        self._result = result
+        self.last: Argmin | None = None
+
+    def _run(self, fn: str, moving: CudaImage, fixed: CudaImage, **kw) -> Argmin:
+        costs = self._result.tensor if self._result is not None else None
+        if costs is not None and costs.numel() < self._grid.numElements():
+            raise ValueError("result tensor is smaller than the grid")
+        self.last = search(fn, moving, fixed, self._grid, costs=costs, **kw)
+        return self.last
+
+    def search(self, fn, moving, fixed, **kw):
+        return self._run(fn, moving, fixed, **kw)
+
+    def search_by_value(self, fn, moving, fixed, **kw):
+        return self._run(fn, moving, fixed, **kw)
+
+    def search_by_value_block(self, fn, numThreads, moving, fixed, **kw):
+        return self._run(fn, moving, fixed, **kw)
+
+    def search_by_value_stream(self, fn, STREAM_BLOCK_DIM, numCores, moving, fixed, **kw):
+        return self._run(fn, moving, fixed, **kw)
+
+    def search_by_reference(self, fn, moving, fixed, **kw):
+        return self._run(fn, moving, fixed, **kw)
+
+    def search_by_reference_stream(self, fn, STREAM_BLOCK_DIM, numCores, moving, fixed, **kw):
+        return self._run(fn, moving, fixed, **kw)

@@ -1,0 +1,102 @@
+"""ctypes binding of ``libcgs_b200.so`` (declared in ``include/cugridsearch_b200.h``).
+
+The library is the product: if it is missing or cannot be loaded this module raises,
+there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcgs_b200.so")
+
+COSTS = {
+    "SAD_AVG": 0, "SAD_AVG_H": 1, "SAD_SUM_T": 2, "SAD_SUM_T_REF": 3, "SQD_REF": 4,
+    "NCC_REF": 5, "SQD_ALT": 6, "NCC_ALT": 7, "MI_ALT": 8, "ZNCC": 9, "MI": 10,
+}
+PIXEL_F32, PIXEL_U8 = 0, 1
+FLAG_NATURAL_ORDER = 1
+
+STATUS = {
+    0: "CGS_SUCCESS", 1: "CGS_ERROR_INVALID_VALUE", 2: "CGS_ERROR_UNSUPPORTED",
+    3: "CGS_ERROR_GRID_TOO_LARGE", 4: "CGS_ERROR_OUT_OF_MEMORY", 5: "CGS_ERROR_CUDA",
+    6: "CGS_ERROR_NO_DEVICE", 7: "CGS_ERROR_DEVICE_TIMEOUT",
+}
+
+# Every symbol the header declares; tests check the library exports all of them.
+EXPORTS = [
+    "cgs_grid_update", "cgs_grid_num_elements", "cgs_grid_point", "cgs_search",
+    "cgs_argmin_f32", "cgs_search_sync", "cgs_status_string", "cgs_last_error", "cgs_version",
+]
+
+
+class CgsImage(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("height", C.c_int32), ("width", C.c_int32),
+                ("channels", C.c_int32), ("pixel", C.c_int32)]
+
+
+class CgsGrid(C.Structure):
+    _fields_ = [("dims", C.c_int32), ("start", C.c_float * 8), ("end", C.c_float * 8),
+                ("resolution", C.c_float * 8), ("count", C.c_float * 8)]
+
+
+class CgsOptions(C.Structure):
+    _fields_ = [("cost", C.c_int32), ("mi_bins", C.c_int32), ("overlap_gate", C.c_float),
+                ("points_per_warp", C.c_int32), ("warps_per_block", C.c_int32), ("flags", C.c_int32)]
+
+
+class CgsArgmin(C.Structure):
+    _fields_ = [("cost", C.c_float), ("valid", C.c_int32), ("index", C.c_int64),
+                ("params", C.c_float * 8), ("status", C.c_int32), ("reserved", C.c_int32)]
+
+
+class CgsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the sm_100a library (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cugridsearch_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        L.cgs_grid_update.restype = C.c_int
+        L.cgs_grid_update.argtypes = [P(CgsGrid), C.c_int32]
+        L.cgs_grid_num_elements.restype = C.c_int
+        L.cgs_grid_num_elements.argtypes = [P(CgsGrid), P(C.c_uint64)]
+        L.cgs_grid_point.restype = C.c_int
+        L.cgs_grid_point.argtypes = [P(CgsGrid), C.c_int64, P(C.c_float)]
+        L.cgs_search.restype = C.c_int
+        L.cgs_search.argtypes = [P(CgsImage), P(CgsImage), P(CgsGrid), P(CgsOptions), C.c_void_p, C.c_void_p,
+                                 C.c_void_p]
+        L.cgs_search_sync.restype = C.c_int
+        L.cgs_search_sync.argtypes = [P(CgsImage), P(CgsImage), P(CgsGrid), P(CgsOptions), C.c_void_p,
+                                      P(CgsArgmin), C.c_void_p]
+        L.cgs_argmin_f32.restype = C.c_int
+        L.cgs_argmin_f32.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.cgs_status_string.restype = C.c_char_p
+        L.cgs_status_string.argtypes = [C.c_int]
+        L.cgs_last_error.restype = C.c_char_p
+        L.cgs_last_error.argtypes = []
+        L.cgs_version.restype = C.c_int32
+        L.cgs_version.argtypes = []
+        _lib = L
+        return L
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = load().cgs_last_error().decode(errors="replace")
+        raise CgsError(status, msg)

@@ -1,0 +1,97 @@
+"""Build the sm_100a shared library ``libcgs_b200.so`` in-tree.
+
+Each ``csrc/*.cu`` is compiled by nvcc for ``sm_100a`` (one object per translation
+unit, in parallel) and linked into ``cugridsearch_b200/libcgs_b200.so`` with the CUDA
+runtime linked statically, so the library loads with nothing but the driver.
+
+Usage: ``python -m cugridsearch_b200.build [--verbose] [--force]``.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libcgs_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2",
+           "-I", CSRC, "-I", INCLUDE]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else (shutil.which("nvcc") or "nvcc")
+
+
+def _sources():
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def _headers():
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))) + \
+        [os.path.join(INCLUDE, "cugridsearch_b200.h")]
+
+
+def _stamp(src: str, extra: list[str]) -> str:
+    h = hashlib.sha256()
+    for f in [src] + _headers():
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    h.update(" ".join(NVFLAGS + ARCH + extra).encode())
+    return h.hexdigest()[:16]
+
+
+def _compile(src: str, verbose: bool, extra: list[str], force: bool) -> str:
+    base = os.path.splitext(os.path.basename(src))[0]
+    obj = os.path.join(OBJ, base + ".o")
+    stamp_file = obj + ".stamp"
+    stamp = _stamp(src, extra)
+    if not force and os.path.exists(obj) and os.path.exists(stamp_file):
+        with open(stamp_file) as fh:
+            if fh.read().strip() == stamp:
+                return obj
+    cmd = [nvcc(), *NVFLAGS, *ARCH, *extra, "-c", src, "-o", obj]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    if verbose and (r.stdout or r.stderr):
+        sys.stderr.write(r.stdout + r.stderr)
+    with open(stamp_file, "w") as fh:
+        fh.write(stamp)
+    return obj
+
+
+def build(verbose: bool = False, force: bool = False, extra: list[str] | None = None) -> str:
+    extra = extra or []
+    os.makedirs(OBJ, exist_ok=True)
+    srcs = _sources()
+    with cf.ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose, extra, force), srcs))
+    newest = max(os.path.getmtime(o) for o in objs)
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+        tmp = LIB + ".tmp"
+        cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-cudart", "static"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose", action="store_true", help="print ptxas register/spill reports")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(verbose=a.verbose, force=a.force))

@@ -1,0 +1,636 @@
+// cgs_search.cu -- C ABI of the sm_100a grid search: argument checks, the reference's
+// grid arithmetic on the host, image staging, launch configuration and the argmin.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cgs_internal.h"
+
+namespace cgs {
+
+// ---------------------------------------------------------------- error reporting
+
+static thread_local std::string g_last_error;
+
+static cgs_status fail(cgs_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+static cgs_status cuda_fail(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(CGS_ERROR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(CGS_ERROR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CGS_CUDA(call, what)                       \
+    do {                                           \
+        cudaError_t e_ = (call);                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// ---------------------------------------------------------------- device memory pool
+
+// One pool per device; scratch is taken and returned on the caller's stream, so
+// concurrent calls on different streams never share it.
+struct DevicePool {
+    std::mutex mu;
+    cudaMemPool_t pool[64] = {};
+};
+static DevicePool g_pools;
+
+static cgs_status get_pool(int dev, cudaMemPool_t *out) {
+    std::lock_guard<std::mutex> lock(g_pools.mu);
+    if (dev < 0 || dev >= 64) return fail(CGS_ERROR_NO_DEVICE, "device ordinal out of range");
+    if (!g_pools.pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p;
+        CGS_CUDA(cudaMemPoolCreate(&p, &props), "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;  // keep freed blocks for reuse by later calls
+        CGS_CUDA(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+        g_pools.pool[dev] = p;
+    }
+    *out = g_pools.pool[dev];
+    return CGS_SUCCESS;
+}
+
+struct DeviceInfo {
+    int dev = -1;
+    int sms = 0;
+    int major = 0;
+};
+
+static cgs_status device_info(DeviceInfo *d) {
+    CGS_CUDA(cudaGetDevice(&d->dev), "cudaGetDevice");
+    CGS_CUDA(cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, d->dev), "cudaDeviceGetAttribute");
+    CGS_CUDA(cudaDeviceGetAttribute(&d->major, cudaDevAttrComputeCapabilityMajor, d->dev), "cudaDeviceGetAttribute");
+    if (d->major != 10) return fail(CGS_ERROR_NO_DEVICE, "this build runs on sm_100 (B200) devices only");
+    return CGS_SUCCESS;
+}
+
+// ---------------------------------------------------------------- grid arithmetic
+
+// CudaGrid dimensional increments and element count exactly as the reference computes
+// them: float count times int increment, truncated to int32 (cudaGridSearch.cuh:89-98, 168-172).
+static void grid_increments(const cgs_grid &g, int32_t inc[8], int64_t *num) {
+    inc[0] = 1;
+    for (int a = 1; a < 8; a++) inc[a] = (a < g.dims) ? (int32_t)(g.count[a - 1] * (float)inc[a - 1]) : 0;
+    int32_t total = 1;
+    for (int a = 0; a < g.dims; a++) total = (int32_t)((float)total * g.count[a]);
+    *num = total;
+}
+
+// The locality order needs the grid to be an exact product of integer counts: then
+// index = sum(i_a * inc[a]) is a bijection onto [0, n).  Fractional counts (the reference
+// allows them, cudaGridSearch_main_mi.cu:304-305) or float products that round make the
+// reference's own decode non-bijective; such grids run in the reference order.
+static bool integral_counts(const cgs_grid &g) {
+    int32_t inc[8];
+    int64_t n;
+    grid_increments(g, inc, &n);
+    int64_t exact = 1;
+    for (int a = 0; a < g.dims; a++) {
+        if (!(g.count[a] >= 1.0f) || g.count[a] != std::floor(g.count[a]) || g.count[a] > 1.0e7f) return false;
+        if (inc[a] != exact) return false;
+        exact *= (int64_t)g.count[a];
+        if (exact > INT32_MAX) return false;
+    }
+    return exact == n;
+}
+
+static bool cost_uses_theta(int cost) {
+    return cost == CGS_COST_SAD_AVG || cost == CGS_COST_SQD_REF || cost == CGS_COST_NCC_REF ||
+           cost == CGS_COST_ZNCC || cost == CGS_COST_MI || cost == CGS_COST_SQD_ALT || cost == CGS_COST_NCC_ALT ||
+           cost == CGS_COST_MI_ALT;
+}
+
+// Host model (double precision) of the sample position of fixed pixel (x, y) for a grid
+// point; used only to choose the evaluation order, never for a cost.
+static void model_map(int cost, const double *q, double cx, double cy, double x, double y, double *mx, double *my) {
+    double h[9];
+    const double th = q[0], sx = q[1], sy = q[2], sh = q[3], tx = q[4], ty = q[5], kx = q[6], ky = q[7];
+    const double c = std::cos(th), s = std::sin(th);
+    if (cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF) {
+        *mx = x + q[0];
+        *my = y + q[1];
+        return;
+    }
+    if (cost == CGS_COST_SAD_AVG_H) {
+        const double z = q[6] * x + q[7] * y + 1.0;
+        *mx = (q[0] * x + q[1] * y + q[2]) / z;
+        *my = (q[3] * x + q[4] * y + q[5]) / z;
+        return;
+    }
+    if (cost == CGS_COST_SAD_AVG) {
+        h[0] = sx * c; h[1] = sy * sh * c - sy * s; h[2] = sx * tx;
+        h[3] = sx * s; h[4] = sy * sh * s + sy * c; h[5] = sy * ty;
+        h[6] = kx; h[7] = ky; h[8] = 1.0;
+    } else {
+        const double a2 = cx * kx + 1, a4 = cx * ky, a6 = c * a2 + a4 * s;
+        const double t5 = sh * a6 - s * a2 + a4 * c;
+        const double b2 = cy * ky + 1, b4 = cy * kx, b6 = s * b2 + b4 * c;
+        const double v5 = sh * b6 + c * b2 - b4 * s;
+        const double d3 = kx * c + ky * s, e5 = sh * d3 + ky * c - kx * s;
+        h[0] = sx * a6; h[1] = sy * t5;
+        h[2] = cx + tx * a2 - cx * sx * a6 - cy * sy * t5 + a4 * ty;
+        h[3] = sx * b6; h[4] = sy * v5;
+        h[5] = cy + ty * b2 - cx * sx * b6 - cy * sy * v5 + b4 * tx;
+        h[6] = sx * d3; h[7] = sy * e5;
+        h[8] = kx * tx + ky * ty - cy * sy * e5 - cx * sx * d3 + 1;
+    }
+    // inverse map through the adjugate (calcNewCoordH)
+    const double w = (h[3] * h[7] - h[4] * h[6]) * x + (h[1] * h[6] - h[0] * h[7]) * y + h[0] * h[4] - h[1] * h[3];
+    const double X = (h[4] * h[8] - h[5] * h[7]) * x + (h[2] * h[7] - h[1] * h[8]) * y + h[1] * h[5] - h[2] * h[4];
+    const double Y = (h[5] * h[6] - h[3] * h[8]) * x + (h[0] * h[8] - h[2] * h[6]) * y + h[2] * h[3] - h[0] * h[5];
+    *mx = X / w;
+    *my = Y / w;
+}
+
+// Evaluation order: axes sorted by how far one step moves the sampled footprint (the
+// largest displacement over the fixed image's corners and centre), smallest first.
+static void locality_order(int cost, const cgs_grid &g, int fw, int fh, int mw, int mh, int32_t perm[8]) {
+    double mid[8] = {0, 1, 1, 0, 0, 0, 0, 0};
+    for (int a = 0; a < g.dims; a++) mid[a] = g.start[a] + 0.5 * (g.count[a] - 1) * g.resolution[a];
+    const double cx = mw * 0.5, cy = mh * 0.5;
+    const double px[5] = {0, (double)fw - 1, 0, (double)fw - 1, 0.5 * fw};
+    const double py[5] = {0, 0, (double)fh - 1, (double)fh - 1, 0.5 * fh};
+    std::vector<std::pair<double, int>> disp;
+    for (int a = 0; a < g.dims; a++) {
+        double d = 0;
+        if (g.count[a] > 1) {
+            double q2[8];
+            memcpy(q2, mid, sizeof(q2));
+            q2[a] += g.resolution[a];
+            for (int k = 0; k < 5; k++) {
+                double x0, y0, x1, y1;
+                model_map(cost, mid, cx, cy, px[k], py[k], &x0, &y0);
+                model_map(cost, q2, cx, cy, px[k], py[k], &x1, &y1);
+                double dd = std::hypot(x1 - x0, y1 - y0);
+                if (!(dd == dd)) dd = 1e30;
+                d = std::max(d, dd);
+            }
+        }
+        disp.push_back({d, a});
+    }
+    std::stable_sort(disp.begin(), disp.end());
+    for (int j = 0; j < 8; j++) perm[j] = j < g.dims ? disp[j].second : j;
+}
+
+// ---------------------------------------------------------------- kernels: staging, argmin
+
+struct PrepParams {
+    const void *mov_src;
+    const void *fix_src;
+    int32_t mov_pix, fix_pix;
+    int32_t mh, mw, fh, fw, c;
+    float *mov_dst;
+    float *fix_dst;
+    int64_t mplane, fplane;
+    int32_t fpitch;
+    unsigned long long *key;
+    unsigned int *done;
+    unsigned int *status;
+};
+
+__device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
+    return pix == CGS_PIXEL_U8 ? (float)static_cast<const uint8_t *>(src)[i] : static_cast<const float *>(src)[i];
+}
+
+// HWC images -> one zero-padded FP32 plane per channel.  Moving planes keep row stride W
+// (the reference's flat indexing) with a zero row after the image; fixed planes use a
+// 16-byte row pitch so rows can be bulk-copied.
+__global__ void prep_kernel(const PrepParams q) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+    if (tid == 0) {
+        *q.key = ~0ull;
+        *q.done = 0u;
+        *q.status = 0u;
+    }
+    const int64_t mtot = q.mplane * q.c;
+    for (int64_t i = tid; i < mtot; i += nthr) {
+        const int c = (int)(i / q.mplane);
+        const int64_t e = i - (int64_t)c * q.mplane;
+        float v = 0.0f;
+        if (e < (int64_t)q.mh * q.mw) v = load_pix(q.mov_src, q.mov_pix, e * q.c + c);
+        q.mov_dst[i] = v;
+    }
+    const int64_t ftot = q.fplane * q.c;
+    for (int64_t i = tid; i < ftot; i += nthr) {
+        const int c = (int)(i / q.fplane);
+        const int64_t e = i - (int64_t)c * q.fplane;
+        const int64_t y = e / q.fpitch, x = e - y * q.fpitch;
+        float v = 0.0f;
+        if (y < q.fh && x < q.fw) v = load_pix(q.fix_src, q.fix_pix, (y * q.fw + x) * q.c + c);
+        q.fix_dst[i] = v;
+    }
+}
+
+__global__ void empty_result_kernel(cgs_argmin *r) {
+    cgs_argmin e;
+    e.cost = __int_as_float(0x7f800000);
+    e.valid = 0;
+    e.index = -1;
+    for (int a = 0; a < 8; a++) e.params[a] = 0.0f;
+    e.status = 0;
+    e.reserved = 0;
+    *r = e;
+}
+
+// Argmin of n floats: grid-stride key min, warp and block reduction, one atomicMin per
+// block; the last block writes the result.  scratch = {key, ticket} preset to all ones.
+__global__ void __launch_bounds__(256) argmin_kernel(const float *__restrict__ v, uint64_t n,
+                                                     unsigned long long *key, unsigned int *ticket,
+                                                     cgs_argmin *out) {
+    __shared__ unsigned long long wk[8];
+    unsigned long long best = ~0ull;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = make_key(__ldg(v + i), (uint32_t)i);
+        best = k < best ? k : best;
+    }
+    best = warp_min_u64(best);
+    if ((threadIdx.x & 31) == 0) wk[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) best = wk[w] < best ? wk[w] : best;
+        if (best != ~0ull) atomicMin(key, best);
+        __threadfence();
+        // the ticket starts at 0xffffffff: the first add returns it, the last returns gridDim - 2
+        const unsigned int t = atomicAdd(ticket, 1u) + 1u;
+        if (t == gridDim.x - 1) {
+            __threadfence();
+            const unsigned long long k = atomicAdd(key, 0ull);
+            cgs_argmin r;
+            r.status = 0;
+            r.reserved = 0;
+            for (int a = 0; a < 8; a++) r.params[a] = 0.0f;
+            if (k == ~0ull) {
+                r.valid = 0;
+                r.index = -1;
+                r.cost = __int_as_float(0x7f800000);
+            } else {
+                r.valid = 1;
+                r.index = (int64_t)(k & 0xffffffffull);
+                r.cost = key_cost(k);
+            }
+            *out = r;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- launch planning
+
+static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+static KernelGetter getter_for(int cost) {
+    switch (cost) {
+        case CGS_COST_SAD_AVG: return kernel_sad_avg;
+        case CGS_COST_SAD_AVG_H: return kernel_sad_avg_h;
+        case CGS_COST_SAD_SUM_T: return kernel_sad_sum_t;
+        case CGS_COST_SAD_SUM_T_REF: return kernel_sad_sum_t_ref;
+        case CGS_COST_SQD_REF: return kernel_sqd_ref;
+        case CGS_COST_NCC_REF: return kernel_ncc_ref;
+        case CGS_COST_ZNCC: return kernel_zncc;
+        case CGS_COST_MI: return kernel_mi;
+        default: return nullptr;
+    }
+}
+
+static cgs_status check_image(const cgs_image *im, const char *name) {
+    if (!im) return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " is null");
+    if (!im->data) return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + "->data is null");
+    if (im->height < 1 || im->width < 1)
+        return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " has an empty size");
+    if (im->pixel != CGS_PIXEL_F32 && im->pixel != CGS_PIXEL_U8)
+        return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " has an unknown pixel type");
+    if (im->channels < 1 || im->channels > 4)
+        return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " must have 1..4 channels");
+    // flat indices are formed in FP32 by the reference; keep them exact
+    if ((int64_t)(im->height + 1) * im->width * im->channels >= (int64_t)1 << 24)
+        return fail(CGS_ERROR_UNSUPPORTED, std::string(name) + " exceeds 2^24 elements");
+    return CGS_SUCCESS;
+}
+
+static cgs_status check_grid(const cgs_grid *g) {
+    if (!g) return fail(CGS_ERROR_INVALID_VALUE, "grid is null");
+    if (g->dims < 1 || g->dims > 8) return fail(CGS_ERROR_INVALID_VALUE, "grid dims must be 1..8");
+    for (int a = 0; a < g->dims; a++) {
+        if (!std::isfinite(g->start[a]) || !std::isfinite(g->end[a]) || !std::isfinite(g->count[a]))
+            return fail(CGS_ERROR_INVALID_VALUE, "grid has a non-finite start, end or count");
+        if (!(g->count[a] >= 1.0f)) return fail(CGS_ERROR_INVALID_VALUE, "grid counts must be >= 1");
+        if (!std::isfinite(g->resolution[a]))
+            return fail(CGS_ERROR_INVALID_VALUE, "grid resolution is not finite (call cgs_grid_update)");
+    }
+    return CGS_SUCCESS;
+}
+
+struct Plan {
+    int G = 2, NW = 16;
+};
+
+static Plan choose_plan(int cost, const cgs_options &o, int mi_bins) {
+    Plan pl;
+    if (cost == CGS_COST_MI) {
+        pl.NW = 8;
+        pl.G = mi_bins > 32 ? 1 : 2;
+    } else if (cost == CGS_COST_ZNCC || cost == CGS_COST_NCC_REF || cost == CGS_COST_SQD_REF) {
+        pl.G = 2;
+    } else {
+        pl.G = 4;
+    }
+    if (o.points_per_warp == 1 || o.points_per_warp == 2 || o.points_per_warp == 4) pl.G = o.points_per_warp;
+    if (o.warps_per_block > 0) pl.NW = o.warps_per_block;
+    return pl;
+}
+
+}  // namespace cgs
+
+using namespace cgs;
+
+// ================================================================= C ABI
+
+extern "C" {
+
+int32_t cgs_version(void) { return 100; }
+
+const char *cgs_status_string(cgs_status s) {
+    switch (s) {
+        case CGS_SUCCESS: return "success";
+        case CGS_ERROR_INVALID_VALUE: return "invalid value";
+        case CGS_ERROR_UNSUPPORTED: return "unsupported";
+        case CGS_ERROR_GRID_TOO_LARGE: return "grid too large";
+        case CGS_ERROR_OUT_OF_MEMORY: return "out of memory";
+        case CGS_ERROR_CUDA: return "CUDA error";
+        case CGS_ERROR_NO_DEVICE: return "no usable device";
+        case CGS_ERROR_DEVICE_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+
+const char *cgs_last_error(void) { return g_last_error.c_str(); }
+
+cgs_status cgs_grid_update(cgs_grid *g, int32_t changed_axis) {
+    if (!g || g->dims < 1 || g->dims > 8) return fail(CGS_ERROR_INVALID_VALUE, "grid is null or dims not in 1..8");
+    const int D = g->dims;
+    auto one = [&](int a, bool changed) {
+        // updateProcess (cudaGridSearch.cuh:241-270): a step below 1e-7 * count collapses
+        // the axis to one sample; the comparison is done in double, as there.
+        if ((double)std::fabs(g->end[a] - g->start[a]) < 1.0e-7 * (double)g->count[a]) g->count[a] = 1;
+        if (g->count[a] == 1) {
+            g->resolution[a] = 2 * (g->end[a] - g->start[a]);
+        } else if (changed) {
+            g->resolution[a] = (float)(int32_t)(g->end[a] - g->start[a]) / (g->count[a] - 1);
+        } else {
+            g->resolution[a] = (g->end[a] - g->start[a]) / (g->count[a] - 1);
+        }
+    };
+    if (changed_axis >= 0 && changed_axis < D) {
+        one(changed_axis, true);
+    } else {
+        for (int a = 0; a < D; a++) one(a, false);
+    }
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_grid_num_elements(const cgs_grid *g, uint64_t *num) {
+    if (!num) return fail(CGS_ERROR_INVALID_VALUE, "num is null");
+    cgs_status s = check_grid(g);
+    if (s != CGS_SUCCESS) return s;
+    int32_t inc[8];
+    int64_t n;
+    grid_increments(*g, inc, &n);
+    *num = n < 0 ? 0 : (uint64_t)n;
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_grid_point(const cgs_grid *g, int64_t index, float out[8]) {
+    if (!out) return fail(CGS_ERROR_INVALID_VALUE, "out is null");
+    cgs_status s = check_grid(g);
+    if (s != CGS_SUCCESS) return s;
+    int32_t inc[8];
+    int64_t n;
+    grid_increments(*g, inc, &n);
+    if (index < 0 || index > INT32_MAX) return fail(CGS_ERROR_INVALID_VALUE, "index out of range");
+    int32_t rem = (int32_t)index, ax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int a = g->dims - 1; a >= 0; a--) {
+        ax[a] = rem / inc[a];
+        rem -= ax[a] * inc[a];
+    }
+    for (int a = 0; a < 8; a++)
+        out[a] = a < g->dims ? std::fmaf((float)ax[a], g->resolution[a], g->start[a]) : 0.0f;
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options *options,
+                      float *costs, cgs_argmin *result, cgs_stream_t stream_) {
+    cudaStream_t stream = (cudaStream_t)stream_;
+    cgs_status s;
+    if ((s = check_image(mov, "moving")) != CGS_SUCCESS) return s;
+    if ((s = check_image(fix, "fixed")) != CGS_SUCCESS) return s;
+    if ((s = check_grid(grid)) != CGS_SUCCESS) return s;
+    if (!options) return fail(CGS_ERROR_INVALID_VALUE, "options is null");
+    if (!result) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
+    const cgs_options o = *options;
+    const int cost = o.cost;
+    if (cost < 0 || cost >= CGS_COST_COUNT) return fail(CGS_ERROR_INVALID_VALUE, "unknown cost");
+    if (mov->channels != fix->channels)
+        return fail(CGS_ERROR_INVALID_VALUE, "moving and fixed images must have the same channel count");
+    const bool eight = !(cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF);
+    if (eight && grid->dims != 8) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs an 8-parameter grid");
+    if (!eight && grid->dims < 2) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs a grid of >= 2 axes");
+    if ((cost == CGS_COST_SAD_AVG_H || cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF) &&
+        fix->channels != 1)
+        return fail(CGS_ERROR_INVALID_VALUE, "this reference functor is single-channel (CudaImage<T>)");
+    int mi_bins = 32;
+    if (cost == CGS_COST_MI) {
+        mi_bins = o.mi_bins == 0 ? 32 : o.mi_bins;
+        if (mi_bins < 2 || mi_bins > 64 || (mi_bins & (mi_bins - 1)))
+            return fail(CGS_ERROR_INVALID_VALUE, "mi_bins must be a power of two in [2, 64]");
+    }
+    KernelGetter getter = getter_for(cost);
+    if (!getter) return fail(CGS_ERROR_UNSUPPORTED, "cost not implemented by this build");
+    const int C = fix->channels;
+    const Plan pl = choose_plan(cost, o, mi_bins);
+    const void *kfn = getter(C, pl.G, pl.NW);
+    if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no kernel for this channel count / tuning");
+
+    DeviceInfo di;
+    if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+
+    int32_t inc[8];
+    int64_t n64;
+    grid_increments(*grid, inc, &n64);
+    if (n64 > INT32_MAX) return fail(CGS_ERROR_GRID_TOO_LARGE, "grid has more than 2^31-1 points");
+    if (n64 <= 0) {
+        empty_result_kernel<<<1, 1, 0, stream>>>(result);
+        CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
+        return CGS_SUCCESS;
+    }
+
+    SearchParams p;
+    memset(&p, 0, sizeof(p));
+    for (int a = 0; a < 8; a++) {
+        p.start[a] = a < grid->dims ? grid->start[a] : 0.0f;
+        p.res[a] = a < grid->dims ? grid->resolution[a] : 0.0f;
+        p.inc[a] = inc[a];
+    }
+    p.dims = grid->dims;
+    p.n = (uint32_t)n64;
+    p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
+    if (!p.natural) {
+        locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
+        for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
+    }
+    if (cost_uses_theta(cost)) {
+        // cos/sin of every axis-0 grid value, with the host libm the reference's CPU path uses
+        const int32_t n0 = grid->dims > 1 ? inc[1] : (int32_t)n64;
+        if (n0 > kMaxTrig) return fail(CGS_ERROR_UNSUPPORTED, "more than 256 values on the rotation axis");
+        for (int32_t i = 0; i < n0; i++) {
+            const float th = std::fmaf((float)i, grid->resolution[0], grid->start[0]);
+            p.trig[i] = make_float2(std::cos(th), std::sin(th));
+        }
+    }
+    p.mov_wf = (float)mov->width;
+    p.mov_hf = (float)mov->height;
+    p.cx = (float)mov->width / 2;
+    p.cy = (float)mov->height / 2;
+    p.mi_bins = mi_bins;
+    p.total_terms = (float)((double)fix->width * fix->height * C);
+    p.gate_n = (float)((double)o.overlap_gate * fix->width * fix->height * C);
+
+    // staged layout
+    const int64_t mplane = round_up((int64_t)(mov->height + 1) * mov->width + 1, 64);
+    const int32_t fpitch = (int32_t)round_up(fix->width, 4);
+    const int64_t fplane = round_up((int64_t)fix->height * fpitch, 64);
+    const int64_t row_bytes = (int64_t)fpitch * 4 * C;
+    int R = (int)std::max<int64_t>(1, 16384 / row_bytes);
+    R = std::min(R, fix->height);
+    p.chunk_rows = R;
+    p.num_chunks = (fix->height + R - 1) / R;
+    const int64_t stage_bytes = (int64_t)R * row_bytes;
+    size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes;
+    if (cost == CGS_COST_MI) smem += (size_t)pl.NW * pl.G * (mi_bins + 1) * (mi_bins + 1) * 4;
+    if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
+
+    const size_t hdr = 256;
+    const size_t bytes = hdr + (size_t)(mplane + fplane) * C * 4;
+    cudaMemPool_t pool;
+    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
+    void *scratch = nullptr;
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, bytes, pool, stream), "cudaMallocFromPoolAsync");
+    char *sb = static_cast<char *>(scratch);
+    p.key = reinterpret_cast<unsigned long long *>(sb);
+    p.done = reinterpret_cast<unsigned int *>(sb + 8);
+    p.status = reinterpret_cast<unsigned int *>(sb + 12);
+    float *mstage = reinterpret_cast<float *>(sb + hdr);
+    float *fstage = mstage + mplane * C;
+    p.mov = Plane{mstage, mov->height, mov->width, C, mov->width, mplane};
+    p.fix = Plane{fstage, fix->height, fix->width, C, fpitch, fplane};
+    p.costs = costs;
+    p.result = result;
+
+    PrepParams q;
+    q.mov_src = mov->data;
+    q.fix_src = fix->data;
+    q.mov_pix = mov->pixel;
+    q.fix_pix = fix->pixel;
+    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
+    q.mov_dst = mstage;
+    q.fix_dst = fstage;
+    q.mplane = mplane;
+    q.fplane = fplane;
+    q.fpitch = fpitch;
+    q.key = p.key;
+    q.done = p.done;
+    q.status = p.status;
+    const int64_t prep_elems = (mplane + fplane) * C;
+    const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
+    prep_kernel<<<prep_blocks, 256, 0, stream>>>(q);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFreeAsync(scratch, stream);
+        return cuda_fail(e, "prep_kernel");
+    }
+
+    const int threads = pl.NW * 32;
+    const uint32_t per_task = (uint32_t)(pl.NW * pl.G);
+    p.num_tasks = (p.n + per_task - 1) / per_task;
+    e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                   cudaSharedmemCarveoutMaxL1);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+    if (e != cudaSuccess || per_sm < 1) {
+        cudaFreeAsync(scratch, stream);
+        return e != cudaSuccess ? cuda_fail(e, "search kernel setup")
+                                : fail(CGS_ERROR_UNSUPPORTED, "search kernel does not fit on an SM");
+    }
+    const uint32_t blocks = std::min<uint32_t>(p.num_tasks, (uint32_t)(di.sms * per_sm));
+    void *args[] = {&p};
+    e = cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, smem, stream);
+    cudaFreeAsync(scratch, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "search kernel launch");
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_search_sync(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid,
+                           const cgs_options *options, float *costs, cgs_argmin *host_result, cgs_stream_t stream_) {
+    if (!host_result) return fail(CGS_ERROR_INVALID_VALUE, "host_result is null");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    DeviceInfo di;
+    cgs_status s;
+    if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+    cudaMemPool_t pool;
+    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
+    void *dres = nullptr;
+    CGS_CUDA(cudaMallocFromPoolAsync(&dres, sizeof(cgs_argmin), pool, stream), "cudaMallocFromPoolAsync");
+    s = cgs_search(mov, fix, grid, options, costs, static_cast<cgs_argmin *>(dres), stream_);
+    if (s == CGS_SUCCESS) {
+        cudaError_t e = cudaMemcpyAsync(host_result, dres, sizeof(cgs_argmin), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) s = cuda_fail(e, "result copy");
+        else if (host_result->status != CGS_SUCCESS) s = fail((cgs_status)host_result->status, "device wait timed out");
+    }
+    cudaFreeAsync(dres, stream);
+    return s;
+}
+
+cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, cgs_stream_t stream_) {
+    cudaStream_t stream = (cudaStream_t)stream_;
+    if (!result) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
+    if (n > 0 && !values) return fail(CGS_ERROR_INVALID_VALUE, "values is null");
+    if (n > 0xffffffffull) return fail(CGS_ERROR_GRID_TOO_LARGE, "more than 2^32 values");
+    DeviceInfo di;
+    cgs_status s;
+    if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+    if (n == 0) {
+        empty_result_kernel<<<1, 1, 0, stream>>>(result);
+        CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
+        return CGS_SUCCESS;
+    }
+    cudaMemPool_t pool;
+    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
+    void *scratch = nullptr;
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, 16, pool, stream), "cudaMallocFromPoolAsync");
+    cudaError_t e = cudaMemsetAsync(scratch, 0xff, 16, stream);
+    const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)di.sms * 4);
+    if (e == cudaSuccess) {
+        argmin_kernel<<<blocks, 256, 0, stream>>>(values, n, static_cast<unsigned long long *>(scratch),
+                                                  reinterpret_cast<unsigned int *>(static_cast<char *>(scratch) + 8),
+                                                  result);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(scratch, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "argmin");
+    return CGS_SUCCESS;
+}
+
+}  // extern "C"

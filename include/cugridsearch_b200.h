@@ -1,0 +1,148 @@
+/*
+ * cugridsearch_b200.h -- C ABI of the B200 (sm_100a) homography grid search.
+ *
+ * The hot path of uncc-visionlab/cuGridSearch is an exhaustive search over an
+ * 8-parameter homography grid for the argmin of an image-similarity cost.  This header
+ * is the drop-in boundary for that path: plain C types, caller-owned device pointers,
+ * status codes instead of exit(), and an explicit CUDA stream on every call.  Each
+ * entry point names the reference interface it replaces (file:line in the reference).
+ *
+ * Threading: every call is safe to issue from several host threads; device scratch is
+ * stream-ordered (taken from a library memory pool on the given stream), so calls on
+ * different streams do not share scratch.  Asynchronous calls return before the GPU
+ * work finishes; results become valid when the stream reaches them.
+ */
+#ifndef CUGRIDSEARCH_B200_H
+#define CUGRIDSEARCH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same type as the CUDA runtime's cudaStream_t; 0 is the legacy default stream. */
+typedef struct CUstream_st *cgs_stream_t;
+
+typedef enum cgs_status {
+    CGS_SUCCESS = 0,
+    CGS_ERROR_INVALID_VALUE = 1,   /* bad descriptor, size or option                        */
+    CGS_ERROR_UNSUPPORTED = 2,     /* valid request this build does not implement           */
+    CGS_ERROR_GRID_TOO_LARGE = 3,  /* more than 2^31 - 1 grid points (reference int32 index) */
+    CGS_ERROR_OUT_OF_MEMORY = 4,   /* device scratch could not be allocated                 */
+    CGS_ERROR_CUDA = 5,            /* a CUDA runtime call failed; see cgs_last_error()       */
+    CGS_ERROR_NO_DEVICE = 6,       /* no sm_100 device, or the kernels cannot load          */
+    CGS_ERROR_DEVICE_TIMEOUT = 7   /* a bounded device-side wait gave up                    */
+} cgs_status;
+
+/* Cost functions.  0-8 reproduce the reference functors; 9-10 are the benchmark costs. */
+typedef enum cgs_cost {
+    CGS_COST_SAD_AVG = 0,       /* averageAbsoluteDifference   src/gpu/cudaErrorFunctions.cuh:31-87    */
+    CGS_COST_SAD_AVG_H = 1,     /* averageAbsoluteDifferenceH  src/gpu/cudaErrorFunctions.cuh:194-224  */
+    CGS_COST_SAD_SUM_T = 2,     /* sumOfAbsoluteDifferences, by value      cudaErrorFunctions.cuh:89-114  */
+    CGS_COST_SAD_SUM_T_REF = 3, /* sumOfAbsoluteDifferences, by reference  cudaErrorFunctions.cuh:171-192 */
+    CGS_COST_SQD_REF = 4,       /* calcSQD      src/gpu/cudaErrorFunctions.cuh:378-446 */
+    CGS_COST_NCC_REF = 5,       /* calcNCC      src/gpu/cudaErrorFunctions.cuh:448-507 */
+    CGS_COST_SQD_ALT = 6,       /* calcSQDAlt   src/gpu/cudaErrorFunctions.cuh:226-300 */
+    CGS_COST_NCC_ALT = 7,       /* calcNCCAlt   src/gpu/cudaErrorFunctions.cuh:302-376 */
+    CGS_COST_MI_ALT = 8,        /* calcMIAlt    src/gpu/cudaErrorFunction_mi.cuh:117-255 (64 bins) */
+    CGS_COST_ZNCC = 9,          /* zero-mean NCC over the calcNCC sampling                 */
+    CGS_COST_MI = 10,           /* -MI x overlap fraction from exact B x B integer counts   */
+    CGS_COST_COUNT = 11
+} cgs_cost;
+
+typedef enum cgs_pixel { CGS_PIXEL_F32 = 0, CGS_PIXEL_U8 = 1 } cgs_pixel;
+
+/* CudaImage<T, C> (include/cudaTensor.cuh:507-596): dims {C, W, H}, HWC row-major,
+ * element (y, x, c) at c + C * (x + W * y).  data is a caller-owned DEVICE pointer. */
+typedef struct cgs_image {
+    const void *data;
+    int32_t height, width, channels; /* channels 1..4 */
+    int32_t pixel;                   /* cgs_pixel */
+} cgs_image;
+
+/* CudaGrid<float, D> (src/gpu/cudaGridSearch.cuh:74-79): the 4 x D matrix of rows
+ * {start, end, resolution, count}.  Counts are floats, as in the reference.  Fill
+ * start/end/count and call cgs_grid_update() before searching (the reference's setters
+ * each call update(), cudaGridSearch.cuh:198-215). */
+typedef struct cgs_grid {
+    int32_t dims; /* 1..8 */
+    float start[8];
+    float end[8];
+    float resolution[8];
+    float count[8];
+} cgs_grid;
+
+typedef struct cgs_options {
+    int32_t cost;            /* cgs_cost */
+    int32_t mi_bins;         /* CGS_COST_MI: power of two in [2, 64]; 0 means 32 */
+    float overlap_gate;      /* CGS_COST_ZNCC / CGS_COST_MI: minimum overlap fraction of the
+                                fixed image (pixels x channels), else the cost is +inf */
+    int32_t points_per_warp; /* 0 = tuned; else 1, 2 or 4 */
+    int32_t warps_per_block; /* 0 = tuned; else 4, 8 or 16 */
+    int32_t flags;           /* CGS_FLAG_* */
+} cgs_options;
+
+/* Evaluate grid points in the reference's index order (axis 0 fastest) instead of the
+ * locality order the library picks.  Results are identical; only speed differs. */
+#define CGS_FLAG_NATURAL_ORDER 1
+
+/* Argmin of a search: the lowest cost, ties broken by the lowest grid index.  NaN and
+ * +inf costs never win (the reference compares with '<', cudaTensor.cuh:256 and
+ * cudaTensorKernels.cuh:45-49); if no cost is finite, valid = 0 and index = -1. */
+typedef struct cgs_argmin {
+    float cost;
+    int32_t valid;
+    int64_t index;
+    float params[8]; /* grid point of index, decoded as CudaGrid::getGridPoint does */
+    int32_t status;  /* cgs_status of the device work (CGS_ERROR_DEVICE_TIMEOUT if a wait gave up) */
+    int32_t reserved;
+} cgs_argmin;
+
+/* CudaGrid::update(changed_axis) -- updateProcess<<<1,1>>> (src/gpu/cudaGridSearch.cuh:100-105,
+ * 235-272), computed on the host with the same FP32 arithmetic. */
+cgs_status cgs_grid_update(cgs_grid *grid, int32_t changed_axis);
+
+/* CudaGrid::numElements (src/gpu/cudaGridSearch.cuh:89-98). */
+cgs_status cgs_grid_num_elements(const cgs_grid *grid, uint64_t *num);
+
+/* CudaGrid::getGridPoint (src/gpu/cudaGridSearch.cuh:189-196) -> gridPointProcess /
+ * indexToGridPoint (:160-187, :274-279): host decode with the device's FP32 result. */
+cgs_status cgs_grid_point(const cgs_grid *grid, int64_t index, float out[8]);
+
+/* CudaGridSearcher::search / search_by_value / search_by_value_block / search_by_value_stream
+ * / search_by_reference[_stream] (src/gpu/cudaGridSearch.cuh:553-556, 562-649, 653-732,
+ * 736-765, 796-827, 831-853) followed by CudaTensor::find_extrema (include/cudaTensor.cuh:215-265)
+ * and CudaGrid::getGridPoint: one fused sm_100a launch evaluates every grid point and
+ * reduces the argmin.
+ *   moving, fixed : device images (moving is sampled, fixed is iterated), as the reference's
+ *                   functor arguments (img_moved, img_fixed).
+ *   costs         : nullable DEVICE array of num_elements floats, costs[i] = cost of grid
+ *                   index i (the reference's result tensor, axis 0 fastest).  The reference
+ *                   kernel also writes costs[num_elements] (bound check '>' at
+ *                   cudaGridSearch.cuh:295); this one does not.
+ *   result        : DEVICE pointer to one cgs_argmin, written when the stream reaches it. */
+cgs_status cgs_search(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
+                      const cgs_options *options, float *costs, cgs_argmin *result, cgs_stream_t stream);
+
+/* CudaTensor<float, D>::find_extrema (include/cudaTensor.cuh:215-265 -> findExtremaProcess /
+ * reduceMin6, include/cudaTensorKernels.cuh:133-220, 247-330): argmin of n device floats
+ * with lowest-index ties.  result is a DEVICE pointer; params are left zero. */
+cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, cgs_stream_t stream);
+
+/* Synchronous convenience: cgs_search on `stream`, then copies the argmin to *host_result. */
+cgs_status cgs_search_sync(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
+                           const cgs_options *options, float *costs, cgs_argmin *host_result,
+                           cgs_stream_t stream);
+
+/* Human-readable status, and the last error message recorded on the calling thread. */
+const char *cgs_status_string(cgs_status status);
+const char *cgs_last_error(void);
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int32_t cgs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUGRIDSEARCH_B200_H */
