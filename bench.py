@@ -38,7 +38,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FLOPS_PER_PIXEL_EVAL = {"ZNCC": 36, "NCC_REF": 36, "SAD_AVG": 32, "MI": 34}
-WORKLOAD = "ncc-single-pair 256x256 f32, zero-mean NCC, 6^8 = 1,679,616 grid points, argmin + cost dump"
+WORKLOADS = {
+    "ncc": "ncc-single-pair 256x256 f32, zero-mean NCC, 6^8 = 1,679,616 grid points, argmin + cost dump",
+    "mi": "mi-single-pair 512x512 u8 (gamma-remapped moving), MI 32x32 bins, 5^8 = 390,625 grid points",
+    "sad": "sad-small 64x64 f32, SAD over the overlap (averageAbsoluteDifference), 4^8 = 65,536 grid points",
+}
+WORKLOAD = WORKLOADS["ncc"]
 METRIC = "homography evals/s"
 UNIT = "grid-point evals/s"
 # DRAM bytes (read + write) of search_kernel per grid point, from the ncu capture summarised in
@@ -171,8 +176,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cost", default="ZNCC")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points-per-warp", type=int, default=0, help="0 = library choice")
     ap.add_argument("--ref-budget", type=float, default=6.0, help="seconds of CPU work per reference step")
     ap.add_argument("--small", action="store_true", help="3^8 grid (for profiling captures)")
+    ap.add_argument("--workload", default="ncc", choices=["ncc", "mi", "sad"],
+                    help="ncc: the headline 256^2 ZNCC pair; mi: 512^2 u8 MI pair; sad: 64^2 SAD pair")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -191,10 +199,14 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    pair = S.config1(S.DEFAULT_SEED + rank)
+    if args.workload == "mi":
+        pair, cost = S.config2(S.DEFAULT_SEED + rank), "MI"
+    elif args.workload == "sad":
+        pair, cost = S.config0(S.DEFAULT_SEED + rank), "SAD_AVG"
+    else:
+        pair, cost = S.config1(S.DEFAULT_SEED + rank), args.cost
     if args.small:
         pair.count[:] = 3
-    cost = args.cost
     stream = torch.cuda.Stream(device=dev)
     mov_h = torch.from_numpy(pair.moving).pin_memory()
     fix_h = torch.from_numpy(pair.fixed).pin_memory()
@@ -211,7 +223,7 @@ def main():
     pix = pair.fixed.shape[0] * pair.fixed.shape[1] * pair.fixed.shape[2]
 
     def step():
-        cgs.search(cost, mov, fix, grid, costs=costs, result=res, stream=stream)
+        cgs.search(cost, mov, fix, grid, costs=costs, result=res, stream=stream, points_per_warp=args.points_per_warp)
 
     def barrier():
         if world > 1:
@@ -296,7 +308,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blob+sinusoid generator, seed "
                                                           f"{S.DEFAULT_SEED}+rank)",
-            "config": {"workload": WORKLOAD, "cost": cost, "grid_points": n, "pixels": pix,
+            "config": {"workload": WORKLOADS[args.workload] + (" (3^8 grid)" if args.small else ""), "cost": cost,
+                       "grid_points": n, "pixels": pix, "points_per_warp": args.points_per_warp or "tuned",
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_total / args.steps},

@@ -199,20 +199,20 @@ class CudaTensor:
 
 
 def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0,
-             warps_per_block: int = 0, natural_order: bool = False) -> CgsOptions:
+             warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool = False) -> CgsOptions:
     if cost not in COSTS:
         raise ValueError(f"unknown cost {cost!r}")
-    return CgsOptions(COSTS[cost], mi_bins, overlap_gate, points_per_warp, warps_per_block,
-                      _abi.FLAG_NATURAL_ORDER if natural_order else 0)
+    flags = (_abi.FLAG_NATURAL_ORDER if natural_order else 0) | (_abi.FLAG_EXACT_SAMPLES if exact_samples else 0)
+    return CgsOptions(COSTS[cost], mi_bins, overlap_gate, points_per_warp, warps_per_block, flags)
 
 
 def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs=None, stream=None,
            mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0, warps_per_block: int = 0,
-           natural_order: bool = False, result=None) -> Argmin | None:
+           natural_order: bool = False, exact_samples: bool = False, result=None) -> Argmin | None:
     """Run one fused search.  With ``result`` (a CUDA uint8 tensor of sizeof(cgs_argmin)
     bytes) the call is asynchronous and returns None; otherwise it synchronises and
     returns the :class:`Argmin`."""
-    opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order)
+    opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples)
     cptr = costs.data_ptr() if costs is not None else None
     s = _stream_handle(stream)
     L = _abi.load()
@@ -231,6 +231,16 @@ def argmin(values, stream=None) -> Argmin:
     out = torch.empty(C.sizeof(CgsArgmin), dtype=torch.uint8, device=values.device)
     check(_abi.load().cgs_argmin_f32(values.data_ptr(), values.numel(), out.data_ptr(), _stream_handle(stream)))
     return Argmin.from_struct(CgsArgmin.from_buffer_copy(out.cpu().numpy().tobytes()))
+
+
+def mi_histogram(moving: CudaImage, fixed: CudaImage, params, bins: int = 32, stream=None) -> np.ndarray:
+    """Joint (fixed bin, moving bin) counts of the MI cost at one parameter vector."""
+    torch = _torch()
+    h = torch.empty(bins * bins, dtype=torch.int32, device=moving.tensor.device)
+    p = (C.c_float * 8)(*[float(np.float32(v)) for v in params])
+    check(_abi.load().cgs_mi_histogram(C.byref(moving.img), C.byref(fixed.img), p, bins, h.data_ptr(),
+                                       _stream_handle(stream)))
+    return h.cpu().numpy().view(np.uint32).reshape(bins, bins)
 
 
 def result_buffer(device=None):

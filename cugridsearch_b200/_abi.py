@@ -18,6 +18,7 @@ COSTS = {
 }
 PIXEL_F32, PIXEL_U8 = 0, 1
 FLAG_NATURAL_ORDER = 1
+FLAG_EXACT_SAMPLES = 2
 
 STATUS = {
     0: "CGS_SUCCESS", 1: "CGS_ERROR_INVALID_VALUE", 2: "CGS_ERROR_UNSUPPORTED",
@@ -29,6 +30,7 @@ STATUS = {
 EXPORTS = [
     "cgs_grid_update", "cgs_grid_num_elements", "cgs_grid_point", "cgs_search",
     "cgs_argmin_f32", "cgs_search_sync", "cgs_status_string", "cgs_last_error", "cgs_version",
+    "cgs_mi_histogram",
 ]
 
 
@@ -86,6 +88,8 @@ def load() -> C.CDLL:
                                       P(CgsArgmin), C.c_void_p]
         L.cgs_argmin_f32.restype = C.c_int
         L.cgs_argmin_f32.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.cgs_mi_histogram.restype = C.c_int
+        L.cgs_mi_histogram.argtypes = [P(CgsImage), P(CgsImage), P(C.c_float), C.c_int32, C.c_void_p, C.c_void_p]
         L.cgs_status_string.restype = C.c_char_p
         L.cgs_status_string.argtypes = [C.c_int]
         L.cgs_last_error.restype = C.c_char_p

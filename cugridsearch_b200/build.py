@@ -23,7 +23,10 @@ LIB = os.path.join(HERE, "libcgs_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2",
+# -fmad=false: no implicit multiply-add contraction.  Every fused operation in the kernels is an
+# explicit fmaf(), so a grid point's arithmetic is the same in every kernel instantiation and
+# results do not depend on the tuning choice.
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
            "-I", CSRC, "-I", INCLUDE]
 
 

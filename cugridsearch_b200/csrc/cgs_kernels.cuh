@@ -12,6 +12,17 @@
 // (per chunk, then per task) and reduced with warp shuffles; the argmin is fused: a
 // 64-bit (cost, index) key per point, warp min, CTA min, one atomicMin per CTA, and
 // the last CTA to finish decodes the winner.
+//
+// Exact decisions, fast samples.  The reference's discrete decisions -- whether a pixel
+// maps inside the moving image and, for MI, the histogram bin of each sample -- are
+// reproduced bit for bit; the sample VALUES only need FP32 accuracy.  So each pixel is
+// mapped with fused multiply-adds and an approximate reciprocal, and a per-grid-point
+// error bound (map_guard) says how far that fast coordinate can be from the reference's
+// correctly rounded one.  A pixel whose fast coordinate is farther than the bound from
+// every decision boundary takes the fast path; the rare rest (a band about a thousandth
+// of a pixel wide around the overlap's edge, samples near an MI bin edge, and every
+// pixel of an ill-conditioned homography) is recomputed with the reference's exact
+// operation sequence.
 #pragma once
 #include "cgs_device.cuh"
 #include "../../include/cugridsearch_b200.h"
@@ -21,6 +32,8 @@ namespace cgs {
 constexpr int kMaxTrig = 256;
 constexpr int kStages = 2;
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s per bounded wait
+constexpr float kMagic = 12582912.0f;            // 1.5 * 2^23: round-down add leaves floor(x) in the mantissa
+constexpr int kMagicBits = 0x4B400000;
 
 struct SearchParams {
     // grid: reference decode tables and the evaluation order
@@ -37,11 +50,13 @@ struct SearchParams {
     float mov_wf, mov_hf;
     float cx, cy;        // parametersToHomography centre: (float)W_m / 2, (float)H_m / 2
     int32_t chunk_rows, num_chunks;
+    int32_t exact_only;  // 1: every pixel takes the exact path (verification)
     // outputs and scratch
     float *costs;
     unsigned long long *key;
     unsigned int *done;
     unsigned int *status;
+    const float *vmax;   // max |moving pixel| (from the staging kernel)
     cgs_argmin *result;
     // cost options
     int32_t mi_bins;
@@ -50,83 +65,177 @@ struct SearchParams {
     float2 trig[kMaxTrig];
 };
 
-// Per-grid-point state of each cost family.
-template <int COST>
-struct Mapper;
+// ---------------------------------------------------------------- the map of a grid point
 
-template <>
-struct Mapper<CGS_COST_SAD_AVG> {
+// General projective map of fixed pixel (x, y) to moving coordinates, in the reference's
+// association: w = ((A*x + B*y) + P) - Q,  X = ((C1*x + C2*y) + R) - S,
+// Y = ((D1*x + D2*y) + T) - U,  mx = X / w,  my = Y / w.  It covers
+//  * calcNewCoordH's adjugate map (cudaImageFunctions.cuh:277-285),
+//  * averageAbsoluteDifferenceH's raw map (cudaErrorFunctions.cuh:205-207): A = H6, B = H7,
+//    P = 1 (the +1.0), C1 = H0, C2 = H1, R = H2, D1 = H3, D2 = H4, T = H5, Q = S = U = 0,
+//  * the translation of sumOfAbsoluteDifferences (:99-100): w = 1, X = x + tx, Y = y + ty.
+// Subtracting a zero and dividing by one are exact, so each form rounds as the reference.
+struct MapCoef {
+    float A, B, P, Q, C1, C2, R, S, D1, D2, T, U;
+};
+
+__device__ __forceinline__ MapCoef coef_from_h(const Homog &h) {
     InvMap m;
-    __device__ void set(const float *q, float2 cs, const SearchParams &) { m.set(h_uncentred(q, cs.x, cs.y)); }
-    __device__ __forceinline__ void map(float x, float y, float &mx, float &my) const { m.map(x, y, mx, my); }
-};
-template <>
-struct Mapper<CGS_COST_SAD_AVG_H> {
-    RawMap m;
-    __device__ void set(const float *q, float2, const SearchParams &) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) m.H[i] = q[i];
+    m.set(h);
+    return MapCoef{m.A, m.B, m.P, m.Q, m.C1, m.C2, m.R, m.S, m.D1, m.D2, m.T, m.U};
+}
+
+template <int COST>
+__device__ __forceinline__ MapCoef make_coef(const float *q, float2 cs, const SearchParams &p) {
+    if constexpr (COST == CGS_COST_SAD_AVG) {
+        return coef_from_h(h_uncentred(q, cs.x, cs.y));
+    } else if constexpr (COST == CGS_COST_SAD_AVG_H) {
+        return MapCoef{q[6], q[7], 1.0f, 0.0f, q[0], q[1], q[2], 0.0f, q[3], q[4], q[5], 0.0f};
+    } else if constexpr (COST == CGS_COST_SAD_SUM_T || COST == CGS_COST_SAD_SUM_T_REF) {
+        return MapCoef{0.0f, 0.0f, 1.0f, 0.0f, 1.0f, 0.0f, q[0], 0.0f, 0.0f, 1.0f, q[1], 0.0f};
+    } else {
+        return coef_from_h(h_centred(q, cs.x, cs.y, p.cx, p.cy));
     }
-    __device__ __forceinline__ void map(float x, float y, float &mx, float &my) const { m.map(x, y, mx, my); }
+}
+
+// The reference's correctly rounded coordinates.
+__device__ __forceinline__ void exact_map(const MapCoef &k, float x, float y, float &mx, float &my) {
+    const float w = xs(xa(xa(xm(k.A, x), xm(k.B, y)), k.P), k.Q);
+    const float X = xs(xa(xa(xm(k.C1, x), xm(k.C2, y)), k.R), k.S);
+    const float Y = xs(xa(xa(xm(k.D1, x), xm(k.D2, y)), k.T), k.U);
+    mx = xd(X, w);
+    my = xd(Y, w);
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Fast-path state of one grid point (registers).
+struct FastMap {
+    float A, B, PQ, C1, C2, RS, D1, D2, TU;  // PQ = P - Q etc.
+    float li_x, lo_x, li_y, lo_y;           // |m - half| < li: clearly inside; > lo: clearly outside
 };
-struct ShiftMap {
-    float tx, ty;
-    __device__ void set(const float *q, float2, const SearchParams &) { tx = q[0]; ty = q[1]; }
-    __device__ __forceinline__ void map(float x, float y, float &mx, float &my) const {
-        mx = xa(x, tx);
-        my = xa(y, ty);
+
+// Error bound of the fast coordinates against the exact ones, over the whole fixed image.
+// With u = 2^-24 and M_w = |A|(W_f-1) + |B|(H_f-1) + |P| + |Q| (M_X, M_Y alike), both the
+// exact and the fast w lie within 4u*M_w of the real-valued w (standard bounds for a sum of
+// four rounded terms), likewise X and Y; the divisions add at most 4u relative (one
+// correctly rounded division; one approximate reciprocal of at most 1 ulp plus a rounded
+// product).  Hence, for |mx| <= B_x = max(W_m, H_m) + 1, where the in/out decisions lie,
+//     |mx_fast - mx_exact| <= 7.2u (M_X + B_x M_w) / w_lo + 4.1u B_x = g_x,
+// w_lo being a lower bound of |w| over the image (w is linear: its extremes are at the
+// corners).  The guard is twice that.  Beyond B_x the bound grows with slope
+// 7.2u M_w / w_lo + 4.1u, which must stay small for "clearly outside" to hold there.  A
+// point whose w may change sign over the image, or whose bound is not small, takes the
+// exact path everywhere.
+__device__ __forceinline__ void map_guard(const MapCoef &k, const SearchParams &p, FastMap &f, float &gx_out,
+                                          float &gy_out) {
+    f.A = k.A; f.B = k.B; f.PQ = k.P - k.Q;
+    f.C1 = k.C1; f.C2 = k.C2; f.RS = k.R - k.S;
+    f.D1 = k.D1; f.D2 = k.D2; f.TU = k.T - k.U;
+    const double u = 5.9604644775390625e-8;  // 2^-24
+    const double X1 = (double)p.fix.w - 1.0, Y1 = (double)p.fix.h - 1.0;
+    const double A = k.A, B = k.B, PQ = (double)k.P - (double)k.Q;
+    const double Mw = fabs(A) * X1 + fabs(B) * Y1 + fabs((double)k.P) + fabs((double)k.Q);
+    const double MX = fabs((double)k.C1) * X1 + fabs((double)k.C2) * Y1 + fabs((double)k.R) + fabs((double)k.S);
+    const double MY = fabs((double)k.D1) * X1 + fabs((double)k.D2) * Y1 + fabs((double)k.T) + fabs((double)k.U);
+    const double w00 = PQ, w10 = A * X1 + PQ, w01 = B * Y1 + PQ, w11 = A * X1 + B * Y1 + PQ;
+    const double wmn = fmin(fmin(w00, w10), fmin(w01, w11));
+    const double wmx = fmax(fmax(w00, w10), fmax(w01, w11));
+    const double werr = 8.0 * u * Mw;
+    bool ok = (wmn > werr) || (wmx < -werr);
+    const double wlo = fmin(fabs(wmn), fabs(wmx)) - werr;
+    const double Bx = fmax((double)p.mov_wf, (double)p.mov_hf) + 1.0;
+    double gx = 0, gy = 0;
+    if (ok) {
+        const double slope = 7.2 * u * Mw / wlo + 4.1 * u;
+        gx = 2.0 * (7.2 * u * (MX + Bx * Mw) / wlo + 4.1 * u * Bx);
+        gy = 2.0 * (7.2 * u * (MY + Bx * Mw) / wlo + 4.1 * u * Bx);
+        ok = slope < 1e-4 && gx < 0.125 && gy < 0.125;
     }
-};
-template <> struct Mapper<CGS_COST_SAD_SUM_T> : ShiftMap {};
-template <> struct Mapper<CGS_COST_SAD_SUM_T_REF> : ShiftMap {};
-struct CentredMap {
-    InvMap m;
-    __device__ void set(const float *q, float2 cs, const SearchParams &p) { m.set(h_centred(q, cs.x, cs.y, p.cx, p.cy)); }
-    __device__ __forceinline__ void map(float x, float y, float &mx, float &my) const { m.map(x, y, mx, my); }
-};
-template <> struct Mapper<CGS_COST_SQD_REF> : CentredMap {};
-template <> struct Mapper<CGS_COST_NCC_REF> : CentredMap {};
-template <> struct Mapper<CGS_COST_ZNCC> : CentredMap {};
-template <> struct Mapper<CGS_COST_MI> : CentredMap {};
+    const float hw = 0.5f * p.mov_wf, hh = 0.5f * p.mov_hf;
+    if (ok && !p.exact_only) {
+        f.li_x = (float)((double)hw - gx);
+        f.lo_x = (float)((double)hw + gx);
+        f.li_y = (float)((double)hh - gy);
+        f.lo_y = (float)((double)hh + gy);
+    } else {  // never clearly inside, never clearly outside: every pixel goes exact
+        f.li_x = f.li_y = -1.0f;
+        f.lo_x = f.lo_y = __int_as_float(0x7f800000);
+    }
+    gx_out = (float)gx;
+    gy_out = (float)gy;
+}
+
+// ---------------------------------------------------------------- costs
 
 // Accumulators: NA floats per grid point plus an integer term count.
 template <int COST> struct AccN { static constexpr int value = 1; };
 template <> struct AccN<CGS_COST_SQD_REF> { static constexpr int value = 3; };
 template <> struct AccN<CGS_COST_NCC_REF> { static constexpr int value = 3; };
 template <> struct AccN<CGS_COST_ZNCC> { static constexpr int value = 5; };
-template <> struct AccN<CGS_COST_MI> { static constexpr int value = 0; };
+template <> struct AccN<CGS_COST_MI> { static constexpr int value = 1; };
 
 constexpr float kZnccShift = 127.5f;  // centre of the [0, 255] range: keeps the one-pass
                                       // variance sums well conditioned
 
-// Accumulate one (fixed value f, moving value v) term.
+// Per-pixel quantities of the fixed value, shared by the G grid points.
+struct FixTerms {
+    float f;    // fixed value
+    float a;    // cost-specific: f/255 (NCC/SQD), f - shift (ZNCC)
+    float b;    // cost-specific: (f/255*f)/255 (NCC/SQD), (f - shift)^2 (ZNCC)
+    int bin;    // MI: fixed bin
+};
+
 template <int COST>
-__device__ __forceinline__ void accumulate(float *a, float f, float v) {
+__device__ __forceinline__ FixTerms fix_terms(float f, const SearchParams &p) {
+    FixTerms t;
+    t.f = f;
+    t.a = 0.0f;
+    t.b = 0.0f;
+    t.bin = 0;
+    if constexpr (COST == CGS_COST_NCC_REF || COST == CGS_COST_SQD_REF) {
+        t.a = xd(f, 255.0f);
+        t.b = xd(xm(t.a, f), 255.0f);
+    } else if constexpr (COST == CGS_COST_ZNCC) {
+        t.a = f - kZnccShift;
+        t.b = t.a * t.a;
+    } else if constexpr (COST == CGS_COST_MI) {
+        const float sB = (float)p.mi_bins * (1.0f / 256.0f);
+        t.bin = min(max((int)floorf(f * sB), 0), p.mi_bins - 1);
+    }
+    return t;
+}
+
+// Accumulate one (fixed, moving value v) term.
+template <int COST>
+__device__ __forceinline__ void accumulate(float *a, const FixTerms &t, float v) {
     if constexpr (COST == CGS_COST_SAD_AVG || COST == CGS_COST_SAD_AVG_H || COST == CGS_COST_SAD_SUM_T ||
                   COST == CGS_COST_SAD_SUM_T_REF) {
-        a[0] += fabsf(xs(v, f));  // |m - f| exactly as the reference forms it
+        a[0] += fabsf(v - t.f);
     } else if constexpr (COST == CGS_COST_NCC_REF) {
-        // calcNCC: i1 += (f/255*f)/255, i2 += t*t, ic += (f/255)*t with t = m/255
-        const float t = xd(v, 255.0f);
-        const float fn = xd(f, 255.0f);
-        a[0] += xd(xm(fn, f), 255.0f);
-        a[1] = fmaf(t, t, a[1]);
-        a[2] = fmaf(fn, t, a[2]);
+        // calcNCC: i1 += (f/255*f)/255, i2 += (m/255)^2, ic += (f/255)(m/255)
+        const float m = v * (1.0f / 255.0f);
+        a[0] += t.b;
+        a[1] = fmaf(m, m, a[1]);
+        a[2] = fmaf(t.a, m, a[2]);
     } else if constexpr (COST == CGS_COST_SQD_REF) {
-        // calcSQD: out += (t - f/255)^2, i1 += t*t, i2 += (f/255*f)/255
-        const float t = xd(v, 255.0f);
-        const float fn = xd(f, 255.0f);
-        const float d = xs(t, fn);
+        // calcSQD: out += (m/255 - f/255)^2, i1 += (m/255)^2, i2 += (f/255*f)/255
+        const float m = v * (1.0f / 255.0f);
+        const float d = m - t.a;
         a[0] = fmaf(d, d, a[0]);
-        a[1] = fmaf(t, t, a[1]);
-        a[2] += xd(xm(fn, f), 255.0f);
+        a[1] = fmaf(m, m, a[1]);
+        a[2] += t.b;
     } else if constexpr (COST == CGS_COST_ZNCC) {
-        const float fs = f - kZnccShift, ms = v - kZnccShift;
-        a[0] += fs;
+        const float ms = v - kZnccShift;
+        a[0] += t.a;
         a[1] += ms;
-        a[2] = fmaf(fs, fs, a[2]);
+        a[2] += t.b;
         a[3] = fmaf(ms, ms, a[3]);
-        a[4] = fmaf(fs, ms, a[4]);
+        a[4] = fmaf(t.a, ms, a[4]);
     }
 }
 
@@ -154,25 +263,40 @@ __device__ __forceinline__ float finalize(const float *a, int n, const SearchPar
     }
 }
 
+// ---------------------------------------------------------------- grid decode
+
 // Ordinal in the evaluation order -> grid index and per-axis indices.
 __device__ __forceinline__ uint32_t ordinal_to_index(const SearchParams &p, uint32_t o, int32_t *ax) {
     if (p.natural) {
         int32_t rem = (int32_t)o;
-        for (int a = p.dims - 1; a >= 0; a--) {  // indexToGridPoint, cudaGridSearch.cuh:174-180
-            ax[a] = rem / p.inc[a];
-            rem -= ax[a] * p.inc[a];
+#pragma unroll
+        for (int a = 7; a >= 0; a--) {  // indexToGridPoint, cudaGridSearch.cuh:174-180
+            if (a < p.dims) {
+                ax[a] = rem / p.inc[a];
+                rem -= ax[a] * p.inc[a];
+            }
         }
         return o;
     }
     uint32_t index = 0;
-    for (int j = 0; j < p.dims; j++) {
-        const int a = p.perm[j];
-        const uint32_t c = (uint32_t)p.ocount[j];
-        const uint32_t q = o / c;
-        const uint32_t r = o - q * c;
-        o = q;
-        ax[a] = (int32_t)r;
-        index += r * (uint32_t)p.inc[a];
+    int32_t r[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        r[j] = 0;
+        if (j < p.dims) {
+            const uint32_t c = (uint32_t)p.ocount[j];
+            const uint32_t q = o / c;
+            r[j] = (int32_t)(o - q * c);
+            o = q;
+            index += (uint32_t)r[j] * (uint32_t)p.inc[p.perm[j]];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        int32_t v = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) v = (p.perm[j] == a && j < p.dims) ? r[j] : v;
+        ax[a] = v;
     }
     return index;
 }
@@ -211,11 +335,19 @@ static __device__ void write_result(const SearchParams &p) {
     *p.result = r;
 }
 
+// ---------------------------------------------------------------- the kernel
+
+// Shared-memory copy of a grid point's exact-path coefficients and guards.
+struct ExactSlot {
+    float P, Q, R, S, T, U, gx, gy;
+};
+
 template <int COST, int C, int G, int NW>
 __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constant__ SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NA = AccN<COST>::value;
     constexpr bool kMI = (COST == CGS_COST_MI);
+    constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     unsigned long long *wbest = reinterpret_cast<unsigned long long *>(smem + 64);
@@ -224,13 +356,22 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
     const int fpitch = p.fix.pitch;
     const int R = p.chunk_rows;
     const int stage_floats = R * fpitch * C;
-    uint32_t *hist_base = reinterpret_cast<uint32_t *>(stages + kStages * stage_floats);
+    ExactSlot *slots = reinterpret_cast<ExactSlot *>(stages + kStages * stage_floats);
+    uint32_t *hist_base = reinterpret_cast<uint32_t *>(slots + NW * G);
     const int B = p.mi_bins;
     const int hstride = B + 1;                 // row stride (bank-conflict padding)
     const int hsize = (B + 1) * (B + 1);       // + a row/column for the marginals
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int fw = p.fix.w, fh = p.fix.h;
+    const int mw = p.mov.w;
+    const int64_t mplane = p.mov.plane;
+    const float *__restrict__ mdata = p.mov.data;
+    const float hw = 0.5f * p.mov_wf, hh = 0.5f * p.mov_hf;
+    const float sB = (float)B * (1.0f / 256.0f);
+    // value-rounding allowance of the MI bin guard: fast and exact bilinear values of the
+    // same coordinates differ by at most 8u * max|v| (bin units, twice for safety)
+    const float gv0 = kMI ? sB * 2.0f * 8.0f * 5.9604645e-8f * (*p.vmax) + 1e-6f : 0.0f;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) mbar_init(&bars[s], 1);
@@ -269,9 +410,10 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
         const uint32_t task = blockIdx.x + k * gridDim.x;
         const uint32_t ord0 = (task * NW + warp) * G;
 
-        Mapper<COST> mp[G];
+        FastMap fm[G];
         uint32_t gidx[G];
         bool gvalid[G];
+        ExactSlot *my_slots = slots + warp * G;
 #pragma unroll
         for (int g = 0; g < G; g++) {
             const uint32_t o = ord0 + g;
@@ -281,22 +423,25 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
             float q[8];
             grid_values(p, ax, q);
             const float2 cs = p.trig[min(ax[0], kMaxTrig - 1)];
-            mp[g].set(q, cs, p);
+            const MapCoef kc = make_coef<COST>(q, cs, p);
+            float gx, gy;
+            map_guard(kc, p, fm[g], gx, gy);
+            if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy};
         }
 
-        float acc[G][NA > 0 ? NA : 1];
+        float acc[G][NA];
         int cnt[G];
 #pragma unroll
         for (int g = 0; g < G; g++) {
             cnt[g] = 0;
 #pragma unroll
-            for (int j = 0; j < (NA > 0 ? NA : 1); j++) acc[g][j] = 0.0f;
+            for (int j = 0; j < NA; j++) acc[g][j] = 0.0f;
         }
         uint32_t *hist = hist_base + (size_t)warp * G * hsize;
         if constexpr (kMI) {
             for (int i = lane; i < G * hsize; i += 32) hist[i] = 0u;
-            __syncwarp();
         }
+        __syncwarp();
 
         for (int ch = 0; ch < p.num_chunks; ch++, it++) {
             const int stage = (int)(it % kStages);
@@ -306,51 +451,108 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
             const int r0 = ch * R;
             const int rows = min(R, fh - r0);
 
-            float part[G][NA > 0 ? NA : 1];
+            float part[G][NA];
 #pragma unroll
             for (int g = 0; g < G; g++)
 #pragma unroll
-                for (int j = 0; j < (NA > 0 ? NA : 1); j++) part[g][j] = 0.0f;
+                for (int j = 0; j < NA; j++) part[g][j] = 0.0f;
 
             int xx = lane, yy = 0;
             while (xx >= fw) { xx -= fw; yy++; }
-            while (yy < rows) {
-                const float xf = (float)xx, yf = (float)(r0 + yy);
-                float fv[C];
-#pragma unroll
-                for (int c = 0; c < C; c++) fv[c] = sfix[c * R * fpitch + yy * fpitch + xx];
+            float xf = (float)xx;
+            float byw[G], byx[G], byy[G];
+            auto set_row = [&](int yrow) {
+                const float yf = (float)(r0 + yrow);
 #pragma unroll
                 for (int g = 0; g < G; g++) {
-                    float mx, my;
-                    mp[g].map(xf, yf, mx, my);
-                    const bool inside = in_image(my, mx, p.mov_wf, p.mov_hf);
-                    if constexpr (COST == CGS_COST_SAD_SUM_T_REF) {
-                        // by-reference SAD: every pixel counts, outside samples read 0
+                    byw[g] = fmaf(fm[g].B, yf, fm[g].PQ);
+                    byx[g] = fmaf(fm[g].C2, yf, fm[g].RS);
+                    byy[g] = fmaf(fm[g].D2, yf, fm[g].TU);
+                }
+            };
+            set_row(yy);
+            while (yy < rows) {
+                FixTerms ft[C];
+#pragma unroll
+                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], p);
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const float w = fmaf(fm[g].A, xf, byw[g]);
+                    const float X = fmaf(fm[g].C1, xf, byx[g]);
+                    const float Y = fmaf(fm[g].D1, xf, byy[g]);
+                    const float rw = rcp_approx(w);
+                    const float mx = X * rw, my = Y * rw;
+                    const float dx = fabsf(mx - hw), dy = fabsf(my - hh);
+                    // 0: clearly outside, 1: clearly inside (fast sample), 2: exact path
+                    int mode = (dx < fm[g].li_x && dy < fm[g].li_y) ? 1
+                                                                     : ((dx > fm[g].lo_x || dy > fm[g].lo_y) ? 0 : 2);
+                    float v[C];
+                    if (mode == 1) {
+                        const float tx = __fadd_rd(mx, kMagic), ty = __fadd_rd(my, kMagic);
+                        const int ix = __float_as_int(tx) - kMagicBits, iy = __float_as_int(ty) - kMagicBits;
+                        const float ax = mx - (tx - kMagic), ay = my - (ty - kMagic);
+                        const int base = ix + mw * iy;
 #pragma unroll
                         for (int c = 0; c < C; c++) {
-                            const float v = inside ? bilinear_in(p.mov.data + c * p.mov.plane, p.mov.w, my, mx) : 0.0f;
-                            accumulate<COST>(part[g], fv[c], v);
-                        }
-                        cnt[g] += C;
-                    } else if (inside) {
-#pragma unroll
-                        for (int c = 0; c < C; c++) {
-                            const float v = bilinear_in(p.mov.data + c * p.mov.plane, p.mov.w, my, mx);
+                            const float *pl = mdata + c * mplane + base;
+                            const float v00 = __ldg(pl), v01 = __ldg(pl + 1);
+                            const float v10 = __ldg(pl + mw), v11 = __ldg(pl + mw + 1);
+                            const float d0 = v01 - v00, d1 = v11 - v10;
+                            const float top = fmaf(ax, d0, v00), bot = fmaf(ax, d1, v10);
+                            v[c] = fmaf(ay, bot - top, top);
                             if constexpr (kMI) {
-                                const float bs = (float)B * (1.0f / 256.0f);
-                                int bf = (int)floorf(fv[c] * bs), bm = (int)floorf(v * bs);
-                                bf = min(max(bf, 0), B - 1);
-                                bm = min(max(bm, 0), B - 1);
-                                atomicAdd(&hist[g * hsize + bf * hstride + bm], 1u);
-                            } else {
-                                accumulate<COST>(part[g], fv[c], v);
+                                // the bin is exact unless the sample could sit on the other side of a
+                                // bin edge (or of a cell edge) from the reference's
+                                const ExactSlot &sl = my_slots[g];
+                                const float t = v[c] * sB;
+                                const float fr = t - floorf(t);
+                                const float Dx = fmaxf(fabsf(d0), fabsf(d1));
+                                const float Dy = fmaxf(fabsf(v10 - v00), fabsf(v11 - v01));
+                                const float gb = sB * (Dx * sl.gx + Dy * sl.gy) + gv0;
+                                const bool near = (fr < gb) || (fr > 1.0f - gb) || (ax < sl.gx) ||
+                                                  (ax > 1.0f - sl.gx) || (ay < sl.gy) || (ay > 1.0f - sl.gy);
+                                if (near) mode = 2;
                             }
                         }
+                    }
+                    if (mode == 2) {
+                        const ExactSlot &sl = my_slots[g];
+                        const MapCoef kc{fm[g].A, fm[g].B, sl.P, sl.Q, fm[g].C1, fm[g].C2, sl.R, sl.S,
+                                         fm[g].D1, fm[g].D2, sl.T, sl.U};
+                        float ex, ey;
+                        exact_map(kc, xf, (float)(r0 + yy), ex, ey);
+                        if (in_image(ey, ex, p.mov_wf, p.mov_hf)) {
+                            mode = 1;
+#pragma unroll
+                            for (int c = 0; c < C; c++) v[c] = bilinear_in(mdata + c * mplane, mw, ey, ex);
+                        } else {
+                            mode = 0;
+                        }
+                    }
+                    if (mode == 1) {
+#pragma unroll
+                        for (int c = 0; c < C; c++) {
+                            if constexpr (kMI) {
+                                const int bm = min(max((int)floorf(v[c] * sB), 0), B - 1);
+                                atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
+                            } else {
+                                accumulate<COST>(part[g], ft[c], v[c]);
+                            }
+                        }
+                        cnt[g] += C;
+                    } else if constexpr (kAllPixels) {
+#pragma unroll
+                        for (int c = 0; c < C; c++) accumulate<COST>(part[g], ft[c], 0.0f);
                         cnt[g] += C;
                     }
                 }
                 xx += 32;
-                while (xx >= fw) { xx -= fw; yy++; }
+                xf += 32.0f;
+                if (xx >= fw) {
+                    do { xx -= fw; yy++; } while (xx >= fw);
+                    xf = (float)xx;
+                    if (yy < rows) set_row(yy);
+                }
             }
 #pragma unroll
             for (int g = 0; g < G; g++)
@@ -424,6 +626,7 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
         }
         kk = warp_min_u64(kk);
         best = kk < best ? kk : best;
+        __syncwarp();  // the slots and histograms are rewritten by the next task
     }
 
     // ---- CTA argmin, one atomic per CTA, last CTA writes the result ----

@@ -198,6 +198,7 @@ struct PrepParams {
     unsigned long long *key;
     unsigned int *done;
     unsigned int *status;
+    float *vmax;  // zeroed before the launch
 };
 
 __device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
@@ -216,13 +217,19 @@ __global__ void prep_kernel(const PrepParams q) {
         *q.status = 0u;
     }
     const int64_t mtot = q.mplane * q.c;
+    unsigned int vmax_bits = 0u;  // max |v| as float bits (non-negative floats order as integers)
     for (int64_t i = tid; i < mtot; i += nthr) {
         const int c = (int)(i / q.mplane);
         const int64_t e = i - (int64_t)c * q.mplane;
         float v = 0.0f;
         if (e < (int64_t)q.mh * q.mw) v = load_pix(q.mov_src, q.mov_pix, e * q.c + c);
         q.mov_dst[i] = v;
+        const float av = fabsf(v);
+        const unsigned int b = (av == av) ? __float_as_uint(av) : 0x7f800000u;
+        vmax_bits = b > vmax_bits ? b : vmax_bits;
     }
+    vmax_bits = __reduce_max_sync(0xffffffffu, vmax_bits);
+    if ((threadIdx.x & 31) == 0 && vmax_bits) atomicMax(reinterpret_cast<unsigned int *>(q.vmax), vmax_bits);
     const int64_t ftot = q.fplane * q.c;
     for (int64_t i = tid; i < ftot; i += nthr) {
         const int c = (int)(i / q.fplane);
@@ -282,6 +289,40 @@ __global__ void __launch_bounds__(256) argmin_kernel(const float *__restrict__ v
                 r.cost = key_cost(k);
             }
             *out = r;
+        }
+    }
+}
+
+// Joint B x B histogram (row = fixed bin, column = moving bin) of the MI sampling at one
+// parameter vector, every sample on the exact path.  hist must be zeroed.
+struct HistParams {
+    Plane mov, fix;
+    float mov_wf, mov_hf;
+    float q[8];
+    float c, s;
+    int bins;
+    uint32_t *hist;
+};
+
+__global__ void hist_kernel(const HistParams hp) {
+    const Plane mov = hp.mov, fix = hp.fix;
+    const float mov_wf = hp.mov_wf, mov_hf = hp.mov_hf;
+    const int bins = hp.bins;
+    uint32_t *hist = hp.hist;
+    const MapCoef k = coef_from_h(h_centred(hp.q, hp.c, hp.s, mov_wf / 2, mov_hf / 2));
+    const float sB = (float)bins * (1.0f / 256.0f);
+    const int64_t npix = (int64_t)fix.w * fix.h;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix; i += (int64_t)gridDim.x * blockDim.x) {
+        const int y = (int)(i / fix.w), x = (int)(i - (int64_t)y * fix.w);
+        float ex, ey;
+        exact_map(k, (float)x, (float)y, ex, ey);
+        if (!in_image(ey, ex, mov_wf, mov_hf)) continue;
+        for (int c = 0; c < fix.c; c++) {
+            const float f = fix.data[c * fix.plane + (int64_t)y * fix.pitch + x];
+            const float v = bilinear_in(mov.data + c * mov.plane, mov.w, ey, ex);
+            const int bf = min(max((int)floorf(f * sB), 0), bins - 1);
+            const int bm = min(max((int)floorf(v * sB), 0), bins - 1);
+            atomicAdd(&hist[bf * bins + bm], 1u);
         }
     }
 }
@@ -485,6 +526,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.dims = grid->dims;
     p.n = (uint32_t)n64;
     p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
+    p.exact_only = (o.flags & CGS_FLAG_EXACT_SAMPLES) ? 1 : 0;
     if (!p.natural) {
         locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
         for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
@@ -516,7 +558,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.chunk_rows = R;
     p.num_chunks = (fix->height + R - 1) / R;
     const int64_t stage_bytes = (int64_t)R * row_bytes;
-    size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes;
+    size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes + (size_t)pl.NW * pl.G * sizeof(ExactSlot);
     if (cost == CGS_COST_MI) smem += (size_t)pl.NW * pl.G * (mi_bins + 1) * (mi_bins + 1) * 4;
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
 
@@ -530,6 +572,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.key = reinterpret_cast<unsigned long long *>(sb);
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
+    p.vmax = reinterpret_cast<float *>(sb + 16);
     float *mstage = reinterpret_cast<float *>(sb + hdr);
     float *fstage = mstage + mplane * C;
     p.mov = Plane{mstage, mov->height, mov->width, C, mov->width, mplane};
@@ -551,10 +594,14 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     q.key = p.key;
     q.done = p.done;
     q.status = p.status;
+    q.vmax = reinterpret_cast<float *>(sb + 16);
     const int64_t prep_elems = (mplane + fplane) * C;
     const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
-    prep_kernel<<<prep_blocks, 256, 0, stream>>>(q);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(scratch, 0, hdr, stream);
+    if (e == cudaSuccess) {
+        prep_kernel<<<prep_blocks, 256, 0, stream>>>(q);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) {
         cudaFreeAsync(scratch, stream);
         return cuda_fail(e, "prep_kernel");
@@ -601,6 +648,66 @@ cgs_status cgs_search_sync(const cgs_image *mov, const cgs_image *fix, const cgs
     }
     cudaFreeAsync(dres, stream);
     return s;
+}
+
+cgs_status cgs_mi_histogram(const cgs_image *mov, const cgs_image *fix, const float params[8], int32_t bins,
+                            uint32_t *hist, cgs_stream_t stream_) {
+    cudaStream_t stream = (cudaStream_t)stream_;
+    cgs_status s;
+    if ((s = check_image(mov, "moving")) != CGS_SUCCESS) return s;
+    if ((s = check_image(fix, "fixed")) != CGS_SUCCESS) return s;
+    if (!params || !hist) return fail(CGS_ERROR_INVALID_VALUE, "params or hist is null");
+    if (mov->channels != fix->channels) return fail(CGS_ERROR_INVALID_VALUE, "channel counts differ");
+    if (bins < 2 || bins > 256 || (bins & (bins - 1)))
+        return fail(CGS_ERROR_INVALID_VALUE, "bins must be a power of two in [2, 256]");
+    DeviceInfo di;
+    if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+    const int C = fix->channels;
+    const int64_t mplane = round_up((int64_t)(mov->height + 1) * mov->width + 1, 64);
+    const int32_t fpitch = (int32_t)round_up(fix->width, 4);
+    const int64_t fplane = round_up((int64_t)fix->height * fpitch, 64);
+    const size_t hdr = 256;
+    cudaMemPool_t pool;
+    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
+    void *scratch = nullptr;
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, hdr + (size_t)(mplane + fplane) * C * 4, pool, stream),
+             "cudaMallocFromPoolAsync");
+    char *sb = static_cast<char *>(scratch);
+    float *mstage = reinterpret_cast<float *>(sb + hdr);
+    float *fstage = mstage + mplane * C;
+    PrepParams q;
+    q.mov_src = mov->data; q.fix_src = fix->data; q.mov_pix = mov->pixel; q.fix_pix = fix->pixel;
+    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
+    q.mov_dst = mstage; q.fix_dst = fstage; q.mplane = mplane; q.fplane = fplane; q.fpitch = fpitch;
+    q.key = reinterpret_cast<unsigned long long *>(sb);
+    q.done = reinterpret_cast<unsigned int *>(sb + 8);
+    q.status = reinterpret_cast<unsigned int *>(sb + 12);
+    q.vmax = reinterpret_cast<float *>(sb + 16);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, hdr, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, (size_t)bins * bins * 4, stream);
+    const int64_t prep_elems = (mplane + fplane) * C;
+    if (e == cudaSuccess) {
+        prep_kernel<<<(int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8), 256, 0, stream>>>(q);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        HistParams hp;
+        hp.mov = Plane{mstage, mov->height, mov->width, C, mov->width, mplane};
+        hp.fix = Plane{fstage, fix->height, fix->width, C, fpitch, fplane};
+        hp.mov_wf = (float)mov->width;
+        hp.mov_hf = (float)mov->height;
+        for (int a = 0; a < 8; a++) hp.q[a] = params[a];
+        hp.c = std::cos(params[0]);  // the host libm, as for cgs_search
+        hp.s = std::sin(params[0]);
+        hp.bins = bins;
+        hp.hist = hist;
+        const int64_t npix = (int64_t)fix->width * fix->height;
+        hist_kernel<<<(int)std::min<int64_t>((npix + 255) / 256, (int64_t)di.sms * 4), 256, 0, stream>>>(hp);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(scratch, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "mi histogram");
+    return CGS_SUCCESS;
 }
 
 cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, cgs_stream_t stream_) {

@@ -86,6 +86,9 @@ typedef struct cgs_options {
 /* Evaluate grid points in the reference's index order (axis 0 fastest) instead of the
  * locality order the library picks.  Results are identical; only speed differs. */
 #define CGS_FLAG_NATURAL_ORDER 1
+/* Take every sample through the reference's exact operation sequence (the kernel otherwise
+ * does so only where a decision is close: see the kernel notes).  For verification. */
+#define CGS_FLAG_EXACT_SAMPLES 2
 
 /* Argmin of a search: the lowest cost, ties broken by the lowest grid index.  NaN and
  * +inf costs never win (the reference compares with '<', cudaTensor.cuh:256 and
@@ -129,6 +132,15 @@ cgs_status cgs_search(const cgs_image *moving, const cgs_image *fixed, const cgs
  * reduceMin6, include/cudaTensorKernels.cuh:133-220, 247-330): argmin of n device floats
  * with lowest-index ties.  result is a DEVICE pointer; params are left zero. */
 cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, cgs_stream_t stream);
+
+/* Joint histogram of the MI cost (CGS_COST_MI sampling: centred homography of params, the
+ * calcNCC pixel loop) at one parameter vector: hist[bf * bins + bm] counts the (pixel, channel)
+ * samples whose fixed value falls in bin bf and moving value in bin bm, bin = floor(v * bins / 256)
+ * clamped.  hist is a DEVICE array of bins * bins uint32 (zeroed by the call).  The counts are
+ * those the search kernel forms at that grid point; the reference forms its 64-bin counts the
+ * same way in calcMIAlt (src/gpu/cudaErrorFunction_mi.cuh:189-195). */
+cgs_status cgs_mi_histogram(const cgs_image *moving, const cgs_image *fixed, const float params[8], int32_t bins,
+                            uint32_t *hist, cgs_stream_t stream);
 
 /* Synchronous convenience: cgs_search on `stream`, then copies the argmin to *host_result. */
 cgs_status cgs_search_sync(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,

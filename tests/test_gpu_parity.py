@@ -154,3 +154,42 @@ def test_argmin_f32(cuda, lib):
     t2 = torch.full((100,), float("nan"), device=cuda)
     r2 = cgs.argmin(t2)
     assert not r2.valid and r2.index == -1
+
+
+@pytest.mark.parametrize("u8", [True, False])
+@pytest.mark.parametrize("bins", [32, 64])
+def test_mi_histogram_counts_exact(cuda, lib, u8, bins):
+    """Joint-histogram counts equal the oracle's (the reference's arithmetic) exactly."""
+    import torch
+    import cugridsearch_b200 as cgs
+    pair = S.small_pair(23, size=48, count=3, cost="MI", u8=u8)
+    mov = cgs.CudaImage(torch.from_numpy(pair.moving).to(cuda))
+    fix = cgs.CudaImage(torch.from_numpy(pair.fixed).to(cuda))
+    F, M = O.Image(pair.fixed), O.Image(pair.moving)
+    rng = np.random.default_rng(5)
+    for k in range(12):
+        params = pair.gt if k == 0 else rng.uniform(pair.lo, pair.hi).astype(np.float32)
+        h = cgs.mi_histogram(mov, fix, params, bins=bins)
+        ho, n = O.histogram("MI", params, M, F, O.opts(bins))
+        np.testing.assert_array_equal(h, ho)
+        assert int(h.sum()) == n
+
+
+@pytest.mark.parametrize("cost", ["MI", "SAD_AVG", "NCC_REF", "ZNCC", "SQD_REF", "SAD_AVG_H"])
+def test_fast_path_decisions_match_exact_path(cuda, lib, cost):
+    """The guarded fast path makes the same decisions as the all-exact path: MI costs are
+    bit-identical (identical histograms), other costs agree to rounding."""
+    pair = S.small_pair(29, size=96, count=3, cost=cost, u8=(cost == "MI"))
+    dg = None
+    if cost == "SAD_AVG_H":
+        dg = ([0.95, -0.05, -4.0, -0.05, 0.95, -4.0, -1e-4, -1e-4], [1.05, 0.05, 4.0, 0.05, 1.05, 4.0, 1e-4, 1e-4],
+              [3] * 8)
+    rf, cf, _ = _gpu_search(cuda, pair, cost, dims_grid=dg)
+    re, ce, _ = _gpu_search(cuda, pair, cost, dims_grid=dg, exact_samples=True)
+    if cost == "MI":
+        np.testing.assert_array_equal(cf, ce)
+    else:
+        fin = np.isfinite(ce)
+        np.testing.assert_array_equal(np.isfinite(cf), fin)
+        assert np.max(np.abs(cf[fin] - ce[fin]) / np.maximum(np.abs(ce[fin]), 1.0)) < 2e-6
+    assert rf.index == re.index or abs(rf.cost - re.cost) <= 2e-6 * max(1.0, abs(re.cost))
