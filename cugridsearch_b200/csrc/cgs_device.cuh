@@ -116,9 +116,13 @@ struct RawMap {
     }
 };
 
-// Staged image: one FP32 plane per channel.  Moving planes keep the reference's row
-// stride (= width) so the flat-index aliasing of CudaImage::valueAt_bilinear holds: a
-// ceil(x) == W tap reads pixel 0 of the next row, and the row after the last is zero.
+// Staged image: one FP32 plane per channel.  The reference addresses a CudaImage with a flat
+// index, so a ceil(x) == W tap reads pixel 0 of the NEXT row and a tap in row H reads past
+// the image (CudaImage::valueAt_bilinear, include/cudaTensor.cuh:561-566 with toIndex :531-534).
+// The staged moving image makes that explicit in a pitched layout: column W of row y holds
+// pixel (0, y + 1) (zero for the last row) and row H is zero, so 2x2 taps at (x, y) and
+// (x + 1, y + 1) read exactly the reference's values for every in-image sample, through plain
+// loads or texture gathers alike.  Planes are stacked: plane c starts at row c * (H + 1).
 struct Plane {
     const float *data;
     int32_t h, w, c;
@@ -131,17 +135,17 @@ __device__ __forceinline__ bool in_image(float y, float x, float wf, float hf) {
     return x >= 0.0f && y >= 0.0f && x < wf && y < hf;
 }
 
-// CudaImage::valueAt_bilinear at an in-image point (include/cudaTensor.cuh:561-575).  The
-// right/bottom taps are read at floor + 1; where the reference's ceil equals floor (an
-// integral coordinate) the weight of that tap is exactly 0, so the value is the same.
-// The staged plane holds a zero row (plus one element) after the image for those reads.
-__device__ __forceinline__ float bilinear_in(const float *__restrict__ pl, int32_t w, float y, float x) {
+// CudaImage::valueAt_bilinear at an in-image point (include/cudaTensor.cuh:561-575), in the
+// reference's operation order.  The right/bottom taps are read at floor + 1; where the
+// reference's ceil equals floor (an integral coordinate) the weight of that tap is exactly 0,
+// so the value is the same.  pl is a staged moving plane with row pitch `pitch`.
+__device__ __forceinline__ float bilinear_in(const float *__restrict__ pl, int32_t pitch, float y, float x) {
     const float fy = floorf(y), fx = floorf(x);
-    const int32_t i = (int32_t)fx + w * (int32_t)fy;
+    const int32_t i = (int32_t)fx + pitch * (int32_t)fy;
     const float tlc = __ldg(pl + i);
     const float trc = __ldg(pl + i + 1);
-    const float blc = __ldg(pl + i + w);
-    const float brc = __ldg(pl + i + w + 1);
+    const float blc = __ldg(pl + i + pitch);
+    const float brc = __ldg(pl + i + pitch + 1);
     const float ax = xs(x, fx), ay = xs(y, fy);
     const float omx = xs(1.0f, ax), omy = xs(1.0f, ay);
     const float top = xa(xm(omx, tlc), xm(ax, trc));

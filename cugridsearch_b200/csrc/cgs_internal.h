@@ -18,20 +18,18 @@ const void *kernel_mi(int C, int G, int NW);
 
 }  // namespace cgs
 
-// Instantiates search_kernel<COST, C, G, NW> for C in {1, 3}, G in {1, 2, 4}.
-#define CGS_DEFINE_KERNEL_GETTER(NAME, COST, NWV)                                              \
+// Instantiates search_kernel<COST, C, G, NW> for C in {1, 3}, G in {1, 2, 4}, NW in {8, 16}.
+#define CGS_KERNEL_CASES(COST, C, NWV)                                                        \
+    if (G == 1) return (const void *)search_kernel<COST, C, 1, NWV>;                          \
+    if (G == 2) return (const void *)search_kernel<COST, C, 2, NWV>;                          \
+    if (G == 4) return (const void *)search_kernel<COST, C, 4, NWV>;
+#define CGS_DEFINE_KERNEL_GETTER(NAME, COST)                                                   \
     namespace cgs {                                                                           \
     const void *NAME(int C, int G, int NW) {                                                  \
-        if (NW != NWV) return nullptr;                                                        \
-        if (C == 1) {                                                                         \
-            if (G == 1) return (const void *)search_kernel<COST, 1, 1, NWV>;                  \
-            if (G == 2) return (const void *)search_kernel<COST, 1, 2, NWV>;                  \
-            if (G == 4) return (const void *)search_kernel<COST, 1, 4, NWV>;                  \
-        } else if (C == 3) {                                                                  \
-            if (G == 1) return (const void *)search_kernel<COST, 3, 1, NWV>;                  \
-            if (G == 2) return (const void *)search_kernel<COST, 3, 2, NWV>;                  \
-            if (G == 4) return (const void *)search_kernel<COST, 3, 4, NWV>;                  \
-        }                                                                                     \
+        if (C == 1 && NW == 16) { CGS_KERNEL_CASES(COST, 1, 16) }                             \
+        if (C == 3 && NW == 16) { CGS_KERNEL_CASES(COST, 3, 16) }                             \
+        if (C == 1 && NW == 8) { CGS_KERNEL_CASES(COST, 1, 8) }                               \
+        if (C == 3 && NW == 8) { CGS_KERNEL_CASES(COST, 3, 8) }                               \
         return nullptr;                                                                       \
     }                                                                                         \
     }

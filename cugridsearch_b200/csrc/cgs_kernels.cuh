@@ -57,6 +57,7 @@ struct SearchParams {
     unsigned int *done;
     unsigned int *status;
     const float *vmax;   // max |moving pixel| (from the staging kernel)
+    cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
     cgs_argmin *result;
     // cost options
     int32_t mi_bins;
@@ -337,17 +338,28 @@ static __device__ void write_result(const SearchParams &p) {
 
 // ---------------------------------------------------------------- the kernel
 
+// MI bin guard of one grid point: coordinate bounds scaled to bin units (sgx, sgy) and the
+// widest fractional tap weight that keeps the sample in its cell (hx, hy).
+struct MiGuard {
+    float sgx, sgy, hx, hy;
+};
+
 // Shared-memory copy of a grid point's exact-path coefficients and guards.
 struct ExactSlot {
     float P, Q, R, S, T, U, gx, gy;
 };
 
+// NW warps per CTA; 512 / (32 NW) CTAs share an SM (two CTAs of 8 warps hide each
+// other's chunk barriers).
 template <int COST, int C, int G, int NW>
-__global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constant__ SearchParams p) {
+__global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_constant__ SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NA = AccN<COST>::value;
     constexpr bool kMI = (COST == CGS_COST_MI);
     constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
+    // taps: one texture gather per sample (fewer instructions); MI, whose extra bin-guard work
+    // leaves less latency tolerance, measured faster with four cached global loads
+    constexpr bool kTexTaps = !kMI;
 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     unsigned long long *wbest = reinterpret_cast<unsigned long long *>(smem + 64);
@@ -357,15 +369,18 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
     const int R = p.chunk_rows;
     const int stage_floats = R * fpitch * C;
     ExactSlot *slots = reinterpret_cast<ExactSlot *>(stages + kStages * stage_floats);
-    uint32_t *hist_base = reinterpret_cast<uint32_t *>(slots + NW * G);
+    // per-task running sums, [warp][g][j][lane]: updated once per chunk (two-level summation)
+    float *totals = reinterpret_cast<float *>(slots + NW * G);
+    uint32_t *hist_base = reinterpret_cast<uint32_t *>(totals + (kMI ? 0 : NW * G * NA * 32));
     const int B = p.mi_bins;
     const int hstride = B + 1;                 // row stride (bank-conflict padding)
     const int hsize = (B + 1) * (B + 1);       // + a row/column for the marginals
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int fw = p.fix.w, fh = p.fix.h;
-    const int mw = p.mov.w;
+    const int mpitch = p.mov.pitch;
     const int64_t mplane = p.mov.plane;
+    const float mrows = (float)(p.mov.h + 1);  // texture rows per plane
     const float *__restrict__ mdata = p.mov.data;
     const float hw = 0.5f * p.mov_wf, hh = 0.5f * p.mov_hf;
     const float sB = (float)B * (1.0f / 256.0f);
@@ -411,6 +426,7 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
         const uint32_t ord0 = (task * NW + warp) * G;
 
         FastMap fm[G];
+        MiGuard mg[G];  // used by the MI instantiations only
         uint32_t gidx[G];
         bool gvalid[G];
         ExactSlot *my_slots = slots + warp * G;
@@ -426,16 +442,22 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
             const MapCoef kc = make_coef<COST>(q, cs, p);
             float gx, gy;
             map_guard(kc, p, fm[g], gx, gy);
+            mg[g].sgx = sB * gx;
+            mg[g].sgy = sB * gy;
+            mg[g].hx = 0.5f - gx;
+            mg[g].hy = 0.5f - gy;
             if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy};
         }
 
-        float acc[G][NA];
+        float *tot = totals + warp * G * NA * 32 + lane;
         int cnt[G];
 #pragma unroll
         for (int g = 0; g < G; g++) {
             cnt[g] = 0;
+            if constexpr (!kMI) {
 #pragma unroll
-            for (int j = 0; j < NA; j++) acc[g][j] = 0.0f;
+                for (int j = 0; j < NA; j++) tot[(g * NA + j) * 32] = 0.0f;
+            }
         }
         uint32_t *hist = hist_base + (size_t)warp * G * hsize;
         if constexpr (kMI) {
@@ -475,68 +497,97 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
                 FixTerms ft[C];
 #pragma unroll
                 for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], p);
+                // 1. fast coordinates and decisions of all G points (independent chains)
+                bool fin[G], amb[G];
+                float mxs[G], mys[G];
 #pragma unroll
                 for (int g = 0; g < G; g++) {
                     const float w = fmaf(fm[g].A, xf, byw[g]);
                     const float X = fmaf(fm[g].C1, xf, byx[g]);
                     const float Y = fmaf(fm[g].D1, xf, byy[g]);
                     const float rw = rcp_approx(w);
-                    const float mx = X * rw, my = Y * rw;
-                    const float dx = fabsf(mx - hw), dy = fabsf(my - hh);
-                    // 0: clearly outside, 1: clearly inside (fast sample), 2: exact path
-                    int mode = (dx < fm[g].li_x && dy < fm[g].li_y) ? 1
-                                                                     : ((dx > fm[g].lo_x || dy > fm[g].lo_y) ? 0 : 2);
-                    float v[C];
-                    if (mode == 1) {
-                        const float tx = __fadd_rd(mx, kMagic), ty = __fadd_rd(my, kMagic);
-                        const int ix = __float_as_int(tx) - kMagicBits, iy = __float_as_int(ty) - kMagicBits;
-                        const float ax = mx - (tx - kMagic), ay = my - (ty - kMagic);
-                        const int base = ix + mw * iy;
+                    mxs[g] = X * rw;
+                    mys[g] = Y * rw;
+                    const float dx = fabsf(mxs[g] - hw), dy = fabsf(mys[g] - hh);
+                    fin[g] = (dx < fm[g].li_x) & (dy < fm[g].li_y);              // clearly inside
+                    amb[g] = !fin[g] & !((dx > fm[g].lo_x) | (dy > fm[g].lo_y)); // undecided: exact path
+                }
+                // 2. taps of all G points: one texture gather returns the 2x2 footprint; the
+                //    gather coordinate is the footprint's centre, (floor + 1) in texel units, so
+                //    the texture unit's fixed-point coordinate rounding cannot change the cell.
+                //    Points not clearly inside read zeros from the border.
+                float v[G][C];
 #pragma unroll
-                        for (int c = 0; c < C; c++) {
+                for (int g = 0; g < G; g++) {
+                    const float tx = __fadd_rd(mxs[g], kMagic), ty = __fadd_rd(mys[g], kMagic);
+                    const float fx = tx - kMagic, fy = ty - kMagic;
+                    const float ax = mxs[g] - fx, ay = mys[g] - fy;
+                    const float u = fin[g] ? fx + 1.0f : -4.0f;
+                    const int base = fin[g] ? (__float_as_int(tx) - kMagicBits) + mpitch * (__float_as_int(ty) - kMagicBits) : 0;
+#pragma unroll
+                    for (int c = 0; c < C; c++) {
+                        float v00, v01, v10, v11;
+                        if constexpr (kTexTaps) {
+                            const float4 t4 = tex2Dgather<float4>(p.mov_tex, u, fy + 1.0f + (float)c * mrows, 0);
+                            // gather order: x = (i0, j1), y = (i1, j1), z = (i1, j0), w = (i0, j0)
+                            v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
+                        } else {
                             const float *pl = mdata + c * mplane + base;
-                            const float v00 = __ldg(pl), v01 = __ldg(pl + 1);
-                            const float v10 = __ldg(pl + mw), v11 = __ldg(pl + mw + 1);
-                            const float d0 = v01 - v00, d1 = v11 - v10;
-                            const float top = fmaf(ax, d0, v00), bot = fmaf(ax, d1, v10);
-                            v[c] = fmaf(ay, bot - top, top);
-                            if constexpr (kMI) {
-                                // the bin is exact unless the sample could sit on the other side of a
-                                // bin edge (or of a cell edge) from the reference's
-                                const ExactSlot &sl = my_slots[g];
-                                const float t = v[c] * sB;
-                                const float fr = t - floorf(t);
-                                const float Dx = fmaxf(fabsf(d0), fabsf(d1));
-                                const float Dy = fmaxf(fabsf(v10 - v00), fabsf(v11 - v01));
-                                const float gb = sB * (Dx * sl.gx + Dy * sl.gy) + gv0;
-                                const bool near = (fr < gb) || (fr > 1.0f - gb) || (ax < sl.gx) ||
-                                                  (ax > 1.0f - sl.gx) || (ay < sl.gy) || (ay > 1.0f - sl.gy);
-                                if (near) mode = 2;
+                            v00 = __ldg(pl); v01 = __ldg(pl + 1);
+                            v10 = __ldg(pl + mpitch); v11 = __ldg(pl + mpitch + 1);
+                        }
+                        const float d0 = v01 - v00, d1 = v11 - v10;
+                        const float top = fmaf(ax, d0, v00), bot = fmaf(ax, d1, v10);
+                        v[g][c] = fmaf(ay, bot - top, top);
+                        if constexpr (kMI) {
+                            // the bin is exact unless the sample could lie across a bin edge (or the
+                            // coordinate across a cell edge) from the reference's sample
+                            const float t = v[g][c] * sB;
+                            const float fr = t - floorf(t);
+                            const float Dx = fmaxf(fabsf(d0), fabsf(d1));
+                            const float Dy = fmaxf(fabsf(v10 - v00), fabsf(v11 - v01));
+                            const float gb = fmaf(Dy, mg[g].sgy, fmaf(Dx, mg[g].sgx, gv0));
+                            const bool near = (fabsf(fr - 0.5f) > 0.5f - gb) | (fabsf(ax - 0.5f) > mg[g].hx) |
+                                              (fabsf(ay - 0.5f) > mg[g].hy);
+                            if (fin[g] & near) {
+                                fin[g] = false;
+                                amb[g] = true;
                             }
                         }
                     }
-                    if (mode == 2) {
-                        const ExactSlot &sl = my_slots[g];
-                        const MapCoef kc{fm[g].A, fm[g].B, sl.P, sl.Q, fm[g].C1, fm[g].C2, sl.R, sl.S,
-                                         fm[g].D1, fm[g].D2, sl.T, sl.U};
-                        float ex, ey;
-                        exact_map(kc, xf, (float)(r0 + yy), ex, ey);
-                        if (in_image(ey, ex, p.mov_wf, p.mov_hf)) {
-                            mode = 1;
+                }
+                // 3. rare: undecided points through the reference's exact operation sequence
+                bool any_amb = false;
 #pragma unroll
-                            for (int c = 0; c < C; c++) v[c] = bilinear_in(mdata + c * mplane, mw, ey, ex);
-                        } else {
-                            mode = 0;
+                for (int g = 0; g < G; g++) any_amb |= amb[g];
+                if (any_amb) {
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        if (amb[g]) {
+                            const ExactSlot &sl = my_slots[g];
+                            const MapCoef kc{fm[g].A, fm[g].B, sl.P, sl.Q, fm[g].C1, fm[g].C2, sl.R, sl.S,
+                                             fm[g].D1, fm[g].D2, sl.T, sl.U};
+                            float ex, ey;
+                            exact_map(kc, xf, (float)(r0 + yy), ex, ey);
+                            if (in_image(ey, ex, p.mov_wf, p.mov_hf)) {
+                                fin[g] = true;
+#pragma unroll
+                                for (int c = 0; c < C; c++) v[g][c] = bilinear_in(mdata + c * mplane, mpitch, ey, ex);
+                            }
                         }
                     }
-                    if (mode == 1) {
+                }
+                // 4. accumulate (predicated)
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    if (fin[g]) {
 #pragma unroll
                         for (int c = 0; c < C; c++) {
                             if constexpr (kMI) {
-                                const int bm = min(max((int)floorf(v[c] * sB), 0), B - 1);
+                                const int bm = min(max((int)floorf(v[g][c] * sB), 0), B - 1);
                                 atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
                             } else {
-                                accumulate<COST>(part[g], ft[c], v[c]);
+                                accumulate<COST>(part[g], ft[c], v[g][c]);
                             }
                         }
                         cnt[g] += C;
@@ -554,10 +605,12 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
                     if (yy < rows) set_row(yy);
                 }
             }
+            if constexpr (!kMI) {
 #pragma unroll
-            for (int g = 0; g < G; g++)
+                for (int g = 0; g < G; g++)
 #pragma unroll
-                for (int j = 0; j < NA; j++) acc[g][j] += part[g][j];
+                    for (int j = 0; j < NA; j++) tot[(g * NA + j) * 32] += part[g][j];
+            }
 
             __syncthreads();
             if (*abort_flag) {
@@ -606,7 +659,7 @@ __global__ void __launch_bounds__(NW * 32, 1) search_kernel(const __grid_constan
             } else {
                 float a[NA];
 #pragma unroll
-                for (int j = 0; j < NA; j++) a[j] = warp_sum(acc[g][j]);
+                for (int j = 0; j < NA; j++) a[j] = warp_sum(tot[(g * NA + j) * 32]);
                 cost = finalize<COST>(a, n, p);
             }
             if (lane == g) my_cost = cost;

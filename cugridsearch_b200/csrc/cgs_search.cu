@@ -66,6 +66,8 @@ struct DeviceInfo {
     int dev = -1;
     int sms = 0;
     int major = 0;
+    int tex_align = 512;
+    int tex_pitch_align = 32;
 };
 
 static cgs_status device_info(DeviceInfo *d) {
@@ -73,6 +75,9 @@ static cgs_status device_info(DeviceInfo *d) {
     CGS_CUDA(cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, d->dev), "cudaDeviceGetAttribute");
     CGS_CUDA(cudaDeviceGetAttribute(&d->major, cudaDevAttrComputeCapabilityMajor, d->dev), "cudaDeviceGetAttribute");
     if (d->major != 10) return fail(CGS_ERROR_NO_DEVICE, "this build runs on sm_100 (B200) devices only");
+    CGS_CUDA(cudaDeviceGetAttribute(&d->tex_align, cudaDevAttrTextureAlignment, d->dev), "cudaDeviceGetAttribute");
+    CGS_CUDA(cudaDeviceGetAttribute(&d->tex_pitch_align, cudaDevAttrTexturePitchAlignment, d->dev),
+             "cudaDeviceGetAttribute");
     return CGS_SUCCESS;
 }
 
@@ -194,7 +199,7 @@ struct PrepParams {
     float *mov_dst;
     float *fix_dst;
     int64_t mplane, fplane;
-    int32_t fpitch;
+    int32_t mpitch, fpitch;
     unsigned long long *key;
     unsigned int *done;
     unsigned int *status;
@@ -205,8 +210,9 @@ __device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
     return pix == CGS_PIXEL_U8 ? (float)static_cast<const uint8_t *>(src)[i] : static_cast<const float *>(src)[i];
 }
 
-// HWC images -> one zero-padded FP32 plane per channel.  Moving planes keep row stride W
-// (the reference's flat indexing) with a zero row after the image; fixed planes use a
+// HWC images -> one zero-padded FP32 plane per channel.  Moving planes are (H + 1) rows of
+// `mpitch` floats: pixels in columns 0..W-1, pixel (0, y + 1) in column W (the reference's
+// flat-index neighbour of (W - 1, y)), zeros elsewhere, a zero row H.  Fixed planes use a
 // 16-byte row pitch so rows can be bulk-copied.
 __global__ void prep_kernel(const PrepParams q) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -221,8 +227,10 @@ __global__ void prep_kernel(const PrepParams q) {
     for (int64_t i = tid; i < mtot; i += nthr) {
         const int c = (int)(i / q.mplane);
         const int64_t e = i - (int64_t)c * q.mplane;
+        const int64_t y = e / q.mpitch, x = e - y * q.mpitch;
         float v = 0.0f;
-        if (e < (int64_t)q.mh * q.mw) v = load_pix(q.mov_src, q.mov_pix, e * q.c + c);
+        if (y < q.mh && x < q.mw) v = load_pix(q.mov_src, q.mov_pix, (y * q.mw + x) * q.c + c);
+        else if (y + 1 < q.mh && x == q.mw) v = load_pix(q.mov_src, q.mov_pix, ((y + 1) * q.mw) * q.c + c);
         q.mov_dst[i] = v;
         const float av = fabsf(v);
         const unsigned int b = (av == av) ? __float_as_uint(av) : 0x7f800000u;
@@ -319,7 +327,7 @@ __global__ void hist_kernel(const HistParams hp) {
         if (!in_image(ey, ex, mov_wf, mov_hf)) continue;
         for (int c = 0; c < fix.c; c++) {
             const float f = fix.data[c * fix.plane + (int64_t)y * fix.pitch + x];
-            const float v = bilinear_in(mov.data + c * mov.plane, mov.w, ey, ex);
+            const float v = bilinear_in(mov.data + c * mov.plane, mov.pitch, ey, ex);
             const int bf = min(max((int)floorf(f * sB), 0), bins - 1);
             const int bm = min(max((int)floorf(v * sB), 0), bins - 1);
             atomicAdd(&hist[bf * bins + bm], 1u);
@@ -330,6 +338,88 @@ __global__ void hist_kernel(const HistParams hp) {
 // ---------------------------------------------------------------- launch planning
 
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Staged layout of a moving/fixed image pair inside one scratch block.
+struct Staging {
+    int32_t mpitch = 0, fpitch = 0;
+    int64_t mplane = 0, fplane = 0;
+    size_t mov_off = 0, fix_off = 0, bytes = 0;
+};
+
+static Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align) {
+    Staging st;
+    const int C = fix.channels;
+    st.mpitch = (int32_t)round_up(mov.width + 1, std::max(1, tex_pitch_align / 4));
+    st.mplane = (int64_t)(mov.height + 1) * st.mpitch;
+    st.fpitch = (int32_t)round_up(fix.width, 4);
+    st.fplane = round_up((int64_t)fix.height * st.fpitch, 64);
+    // offsets from a tex_align-aligned origin; the allocation carries tex_align bytes of slack
+    st.mov_off = (size_t)round_up(256, tex_align);
+    st.fix_off = st.mov_off + (size_t)round_up(st.mplane * C * 4, 256);
+    st.bytes = st.fix_off + (size_t)st.fplane * C * 4 + (size_t)tex_align;
+    return st;
+}
+
+// Origin of a staging block: the first tex_align boundary at or after the allocation.
+static char *staging_origin(void *scratch, int tex_align) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(scratch);
+    return reinterpret_cast<char *>((a + (uintptr_t)tex_align - 1) / (uintptr_t)tex_align * (uintptr_t)tex_align);
+}
+
+// Texture objects over staged moving images, cached by (device, address, geometry): scratch
+// comes from the library's pool, so steady workloads reuse the same few blocks.  Each entry
+// records an event after every kernel that reads it; an entry is destroyed only after its
+// event completes.  The mutex is held from lookup through launch and event record.
+struct TexEntry {
+    int dev;
+    const void *ptr;
+    int w, h;
+    size_t pitch;
+    cudaTextureObject_t tex;
+    cudaEvent_t last;
+};
+static std::mutex g_tex_mu;
+static std::vector<TexEntry> g_tex;
+constexpr size_t kTexCacheMax = 64;
+
+static cgs_status texture_for(int dev, const float *ptr, int w, int h, size_t pitch_bytes, TexEntry **out) {
+    for (auto &e : g_tex)
+        if (e.dev == dev && e.ptr == ptr && e.w == w && e.h == h && e.pitch == pitch_bytes) {
+            *out = &e;
+            return CGS_SUCCESS;
+        }
+    if (g_tex.size() >= kTexCacheMax) {
+        TexEntry &old = g_tex.front();
+        cudaEventSynchronize(old.last);
+        cudaDestroyTextureObject(old.tex);
+        cudaEventDestroy(old.last);
+        g_tex.erase(g_tex.begin());
+    }
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = const_cast<float *>(ptr);
+    rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+    rd.res.pitch2D.width = (size_t)w;
+    rd.res.pitch2D.height = (size_t)h;
+    rd.res.pitch2D.pitchInBytes = pitch_bytes;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;  // outside reads 0
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    TexEntry e{dev, ptr, w, h, pitch_bytes, 0, nullptr};
+    CGS_CUDA(cudaCreateTextureObject(&e.tex, &rd, &td, nullptr), "cudaCreateTextureObject");
+    cudaError_t err = cudaEventCreateWithFlags(&e.last, cudaEventDisableTiming);
+    if (err != cudaSuccess) {
+        cudaDestroyTextureObject(e.tex);
+        return cuda_fail(err, "cudaEventCreateWithFlags");
+    }
+    g_tex.push_back(e);
+    *out = &g_tex.back();
+    return CGS_SUCCESS;
+}
 
 static KernelGetter getter_for(int cost) {
     switch (cost) {
@@ -354,6 +444,8 @@ static cgs_status check_image(const cgs_image *im, const char *name) {
         return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " has an unknown pixel type");
     if (im->channels < 1 || im->channels > 4)
         return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " must have 1..4 channels");
+    if ((int64_t)(im->height + 1) * im->channels > 65000 || im->width + 1 > 131000)
+        return fail(CGS_ERROR_UNSUPPORTED, std::string(name) + " exceeds the 2-D texture limits");
     // flat indices are formed in FP32 by the reference; keep them exact
     if ((int64_t)(im->height + 1) * im->width * im->channels >= (int64_t)1 << 24)
         return fail(CGS_ERROR_UNSUPPORTED, std::string(name) + " exceeds 2^24 elements");
@@ -377,13 +469,20 @@ struct Plan {
     int G = 2, NW = 16;
 };
 
+static int accumulators(int cost) {
+    switch (cost) {
+        case CGS_COST_SQD_REF:
+        case CGS_COST_NCC_REF: return AccN<CGS_COST_NCC_REF>::value;
+        case CGS_COST_ZNCC: return AccN<CGS_COST_ZNCC>::value;
+        default: return 1;
+    }
+}
+
 static Plan choose_plan(int cost, const cgs_options &o, int mi_bins) {
     Plan pl;
     if (cost == CGS_COST_MI) {
-        pl.NW = 8;
+        pl.NW = mi_bins > 32 ? 8 : 16;
         pl.G = mi_bins > 32 ? 1 : 2;
-    } else if (cost == CGS_COST_ZNCC || cost == CGS_COST_NCC_REF || cost == CGS_COST_SQD_REF) {
-        pl.G = 2;
     } else {
         pl.G = 4;
     }
@@ -549,10 +648,8 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.gate_n = (float)((double)o.overlap_gate * fix->width * fix->height * C);
 
     // staged layout
-    const int64_t mplane = round_up((int64_t)(mov->height + 1) * mov->width + 1, 64);
-    const int32_t fpitch = (int32_t)round_up(fix->width, 4);
-    const int64_t fplane = round_up((int64_t)fix->height * fpitch, 64);
-    const int64_t row_bytes = (int64_t)fpitch * 4 * C;
+    const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align);
+    const int64_t row_bytes = (int64_t)st.fpitch * 4 * C;
     int R = (int)std::max<int64_t>(1, 16384 / row_bytes);
     R = std::min(R, fix->height);
     p.chunk_rows = R;
@@ -560,23 +657,22 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     const int64_t stage_bytes = (int64_t)R * row_bytes;
     size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes + (size_t)pl.NW * pl.G * sizeof(ExactSlot);
     if (cost == CGS_COST_MI) smem += (size_t)pl.NW * pl.G * (mi_bins + 1) * (mi_bins + 1) * 4;
+    else smem += (size_t)pl.NW * pl.G * accumulators(cost) * 32 * 4;
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
 
-    const size_t hdr = 256;
-    const size_t bytes = hdr + (size_t)(mplane + fplane) * C * 4;
     cudaMemPool_t pool;
     if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
     void *scratch = nullptr;
-    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, bytes, pool, stream), "cudaMallocFromPoolAsync");
-    char *sb = static_cast<char *>(scratch);
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes, pool, stream), "cudaMallocFromPoolAsync");
+    char *sb = staging_origin(scratch, di.tex_align);
     p.key = reinterpret_cast<unsigned long long *>(sb);
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
     p.vmax = reinterpret_cast<float *>(sb + 16);
-    float *mstage = reinterpret_cast<float *>(sb + hdr);
-    float *fstage = mstage + mplane * C;
-    p.mov = Plane{mstage, mov->height, mov->width, C, mov->width, mplane};
-    p.fix = Plane{fstage, fix->height, fix->width, C, fpitch, fplane};
+    float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
+    float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
+    p.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};
+    p.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
     p.costs = costs;
     p.result = result;
 
@@ -588,16 +684,17 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
     q.mov_dst = mstage;
     q.fix_dst = fstage;
-    q.mplane = mplane;
-    q.fplane = fplane;
-    q.fpitch = fpitch;
+    q.mplane = st.mplane;
+    q.fplane = st.fplane;
+    q.mpitch = st.mpitch;
+    q.fpitch = st.fpitch;
     q.key = p.key;
     q.done = p.done;
     q.status = p.status;
     q.vmax = reinterpret_cast<float *>(sb + 16);
-    const int64_t prep_elems = (mplane + fplane) * C;
+    const int64_t prep_elems = (st.mplane + st.fplane) * C;
     const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, hdr, stream);
+    cudaError_t e = cudaMemsetAsync(sb, 0, 256, stream);
     if (e == cudaSuccess) {
         prep_kernel<<<prep_blocks, 256, 0, stream>>>(q);
         e = cudaGetLastError();
@@ -622,8 +719,18 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     }
     const uint32_t blocks = std::min<uint32_t>(p.num_tasks, (uint32_t)(di.sms * per_sm));
     void *args[] = {&p};
-    e = cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, smem, stream);
+    {
+        std::lock_guard<std::mutex> lock(g_tex_mu);
+        TexEntry *te = nullptr;
+        s = texture_for(di.dev, mstage, mov->width + 1, C * (mov->height + 1), (size_t)st.mpitch * 4, &te);
+        if (s == CGS_SUCCESS) {
+            p.mov_tex = te->tex;
+            e = cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, smem, stream);
+            if (e == cudaSuccess) e = cudaEventRecord(te->last, stream);
+        }
+    }
     cudaFreeAsync(scratch, stream);
+    if (s != CGS_SUCCESS) return s;
     if (e != cudaSuccess) return cuda_fail(e, "search kernel launch");
     return CGS_SUCCESS;
 }
@@ -663,37 +770,34 @@ cgs_status cgs_mi_histogram(const cgs_image *mov, const cgs_image *fix, const fl
     DeviceInfo di;
     if ((s = device_info(&di)) != CGS_SUCCESS) return s;
     const int C = fix->channels;
-    const int64_t mplane = round_up((int64_t)(mov->height + 1) * mov->width + 1, 64);
-    const int32_t fpitch = (int32_t)round_up(fix->width, 4);
-    const int64_t fplane = round_up((int64_t)fix->height * fpitch, 64);
-    const size_t hdr = 256;
+    const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align);
     cudaMemPool_t pool;
     if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
     void *scratch = nullptr;
-    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, hdr + (size_t)(mplane + fplane) * C * 4, pool, stream),
-             "cudaMallocFromPoolAsync");
-    char *sb = static_cast<char *>(scratch);
-    float *mstage = reinterpret_cast<float *>(sb + hdr);
-    float *fstage = mstage + mplane * C;
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes, pool, stream), "cudaMallocFromPoolAsync");
+    char *sb = staging_origin(scratch, di.tex_align);
+    float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
+    float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
     PrepParams q;
     q.mov_src = mov->data; q.fix_src = fix->data; q.mov_pix = mov->pixel; q.fix_pix = fix->pixel;
     q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
-    q.mov_dst = mstage; q.fix_dst = fstage; q.mplane = mplane; q.fplane = fplane; q.fpitch = fpitch;
+    q.mov_dst = mstage; q.fix_dst = fstage; q.mplane = st.mplane; q.fplane = st.fplane;
+    q.mpitch = st.mpitch; q.fpitch = st.fpitch;
     q.key = reinterpret_cast<unsigned long long *>(sb);
     q.done = reinterpret_cast<unsigned int *>(sb + 8);
     q.status = reinterpret_cast<unsigned int *>(sb + 12);
     q.vmax = reinterpret_cast<float *>(sb + 16);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, hdr, stream);
+    cudaError_t e = cudaMemsetAsync(sb, 0, 256, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, (size_t)bins * bins * 4, stream);
-    const int64_t prep_elems = (mplane + fplane) * C;
+    const int64_t prep_elems = (st.mplane + st.fplane) * C;
     if (e == cudaSuccess) {
         prep_kernel<<<(int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8), 256, 0, stream>>>(q);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
         HistParams hp;
-        hp.mov = Plane{mstage, mov->height, mov->width, C, mov->width, mplane};
-        hp.fix = Plane{fstage, fix->height, fix->width, C, fpitch, fplane};
+        hp.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};
+        hp.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
         hp.mov_wf = (float)mov->width;
         hp.mov_hf = (float)mov->height;
         for (int a = 0; a < 8; a++) hp.q[a] = params[a];

@@ -1,3 +1,3 @@
 // Kernel instantiations for CGS_COST_NCC_REF (one translation unit per cost, compiled in parallel).
 #include "cgs_internal.h"
-CGS_DEFINE_KERNEL_GETTER(kernel_ncc_ref, CGS_COST_NCC_REF, 16)
+CGS_DEFINE_KERNEL_GETTER(kernel_ncc_ref, CGS_COST_NCC_REF)

@@ -1,3 +1,3 @@
 // Kernel instantiations for CGS_COST_SQD_REF (one translation unit per cost, compiled in parallel).
 #include "cgs_internal.h"
-CGS_DEFINE_KERNEL_GETTER(kernel_sqd_ref, CGS_COST_SQD_REF, 16)
+CGS_DEFINE_KERNEL_GETTER(kernel_sqd_ref, CGS_COST_SQD_REF)

@@ -1,3 +1,3 @@
 // Kernel instantiations for CGS_COST_ZNCC (one translation unit per cost, compiled in parallel).
 #include "cgs_internal.h"
-CGS_DEFINE_KERNEL_GETTER(kernel_zncc, CGS_COST_ZNCC, 16)
+CGS_DEFINE_KERNEL_GETTER(kernel_zncc, CGS_COST_ZNCC)
