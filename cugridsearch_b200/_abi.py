@@ -30,7 +30,7 @@ STATUS = {
 EXPORTS = [
     "cgs_grid_update", "cgs_grid_num_elements", "cgs_grid_point", "cgs_search",
     "cgs_argmin_f32", "cgs_search_sync", "cgs_status_string", "cgs_last_error", "cgs_version",
-    "cgs_mi_histogram",
+    "cgs_mi_histogram", "cgs_search_noalloc",
 ]
 
 
@@ -83,6 +83,9 @@ def load() -> C.CDLL:
         L.cgs_search.restype = C.c_int
         L.cgs_search.argtypes = [P(CgsImage), P(CgsImage), P(CgsGrid), P(CgsOptions), C.c_void_p, C.c_void_p,
                                  C.c_void_p]
+        L.cgs_search_noalloc.restype = C.c_int
+        L.cgs_search_noalloc.argtypes = [P(CgsImage), P(CgsImage), P(CgsGrid), P(CgsOptions), C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
         L.cgs_search_sync.restype = C.c_int
         L.cgs_search_sync.argtypes = [P(CgsImage), P(CgsImage), P(CgsGrid), P(CgsOptions), C.c_void_p,
                                       P(CgsArgmin), C.c_void_p]

@@ -16,6 +16,16 @@ const void *kernel_ncc_ref(int C, int G, int NW);
 const void *kernel_zncc(int C, int G, int NW);
 const void *kernel_mi(int C, int G, int NW);
 
+// Plain-load (no texture object) variants at 4 points per warp and 16 warps, for the
+// allocation-free entry point.
+const void *kernel_sad_avg_loads(int C);
+const void *kernel_sad_avg_h_loads(int C);
+const void *kernel_sad_sum_t_loads(int C);
+const void *kernel_sad_sum_t_ref_loads(int C);
+const void *kernel_sqd_ref_loads(int C);
+const void *kernel_ncc_ref_loads(int C);
+const void *kernel_zncc_loads(int C);
+
 }  // namespace cgs
 
 // Instantiates search_kernel<COST, C, G, NW> for C in {1, 3}, G in {1, 2, 4}, NW in {8, 16}.
@@ -30,6 +40,15 @@ const void *kernel_mi(int C, int G, int NW);
         if (C == 3 && NW == 16) { CGS_KERNEL_CASES(COST, 3, 16) }                             \
         if (C == 1 && NW == 8) { CGS_KERNEL_CASES(COST, 1, 8) }                               \
         if (C == 3 && NW == 8) { CGS_KERNEL_CASES(COST, 3, 8) }                               \
+        return nullptr;                                                                       \
+    }                                                                                         \
+    }
+
+#define CGS_DEFINE_LOADS_GETTER(NAME, COST)                                                    \
+    namespace cgs {                                                                           \
+    const void *NAME(int C) {                                                                 \
+        if (C == 1) return (const void *)search_kernel<COST, 1, 4, 16, false>;                \
+        if (C == 3) return (const void *)search_kernel<COST, 3, 4, 16, false>;                \
         return nullptr;                                                                       \
     }                                                                                         \
     }

@@ -351,7 +351,7 @@ struct ExactSlot {
 
 // NW warps per CTA; 512 / (32 NW) CTAs share an SM (two CTAs of 8 warps hide each
 // other's chunk barriers).
-template <int COST, int C, int G, int NW>
+template <int COST, int C, int G, int NW, bool TEX = (COST != CGS_COST_MI)>
 __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_constant__ SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NA = AccN<COST>::value;
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
     constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
     // taps: one texture gather per sample (fewer instructions); MI, whose extra bin-guard work
     // leaves less latency tolerance, measured faster with four cached global loads
-    constexpr bool kTexTaps = !kMI;
+    constexpr bool kTexTaps = TEX;
 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     unsigned long long *wbest = reinterpret_cast<unsigned long long *>(smem + 64);

@@ -757,6 +757,224 @@ cgs_status cgs_search_sync(const cgs_image *mov, const cgs_image *fix, const cgs
     return s;
 }
 
+// ================================================================= allocation-free search
+//
+// Some callers cannot allocate device memory while they run: a real-time or streaming loop
+// that reserves its whole memory budget up front (an allocation there can block on an
+// implicit synchronisation or fail once a caching allocator such as PyTorch's holds nearly
+// all free memory), or a host that owns device memory through its own pool and forbids
+// other allocations.  cgs_search takes its scratch from a stream-ordered pool;
+// cgs_search_noalloc takes it from the fixed array below instead and calls no allocation
+// routine at all.  Every GPU that loads this library holds the array until the process
+// exits.
+
+}  // extern "C"
+
+namespace cgs {
+
+// Maximum scratch of an allocation-free search: the staged moving and fixed images
+// (C planes of (H_m + 1) x pitch and H_f x pitch floats) plus a 256-byte header.
+constexpr size_t kStaticScratchBytes = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mu;
+static char *g_static_ptr[64] = {};
+
+// The device address of g_static_scratch on the current device.  In host code the array's
+// name stands for a host-side shadow, not a device address, so it is looked up once per
+// device with cudaGetSymbolAddress while that device is current.
+static cgs_status static_scratch(int dev, char **out) {
+    if (dev < 0 || dev >= 64) return fail(CGS_ERROR_NO_DEVICE, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void *ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+        g_static_ptr[dev] = static_cast<char *>(ptr);
+    }
+    *out = g_static_ptr[dev];
+    return CGS_SUCCESS;
+}
+
+static const void *loads_kernel_for(int cost, int C) {
+    switch (cost) {
+        case CGS_COST_SAD_AVG: return kernel_sad_avg_loads(C);
+        case CGS_COST_SAD_AVG_H: return kernel_sad_avg_h_loads(C);
+        case CGS_COST_SAD_SUM_T: return kernel_sad_sum_t_loads(C);
+        case CGS_COST_SAD_SUM_T_REF: return kernel_sad_sum_t_ref_loads(C);
+        case CGS_COST_SQD_REF: return kernel_sqd_ref_loads(C);
+        case CGS_COST_NCC_REF: return kernel_ncc_ref_loads(C);
+        case CGS_COST_ZNCC: return kernel_zncc_loads(C);
+        default: return nullptr;
+    }
+}
+
+}  // namespace cgs
+
+extern "C" {
+
+cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid,
+                              const cgs_options *options, float *costs, cgs_argmin *result, cgs_stream_t stream_) {
+    cudaStream_t stream = (cudaStream_t)stream_;
+    cgs_status s;
+    if ((s = check_image(mov, "moving")) != CGS_SUCCESS) return s;
+    if ((s = check_image(fix, "fixed")) != CGS_SUCCESS) return s;
+    if ((s = check_grid(grid)) != CGS_SUCCESS) return s;
+    if (!options) return fail(CGS_ERROR_INVALID_VALUE, "options is null");
+    if (!result) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
+    const cgs_options o = *options;
+    const int cost = o.cost;
+    if (cost < 0 || cost >= CGS_COST_COUNT) return fail(CGS_ERROR_INVALID_VALUE, "unknown cost");
+    if (mov->channels != fix->channels)
+        return fail(CGS_ERROR_INVALID_VALUE, "moving and fixed images must have the same channel count");
+    const bool eight = !(cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF);
+    if (eight && grid->dims != 8) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs an 8-parameter grid");
+    if (!eight && grid->dims < 2) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs a grid of >= 2 axes");
+    if ((cost == CGS_COST_SAD_AVG_H || cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF) &&
+        fix->channels != 1)
+        return fail(CGS_ERROR_INVALID_VALUE, "this reference functor is single-channel (CudaImage<T>)");
+    int mi_bins = 32;
+    if (cost == CGS_COST_MI) {
+        mi_bins = o.mi_bins == 0 ? 32 : o.mi_bins;
+        if (mi_bins < 2 || mi_bins > 64 || (mi_bins & (mi_bins - 1)))
+            return fail(CGS_ERROR_INVALID_VALUE, "mi_bins must be a power of two in [2, 64]");
+    }
+    const int C = fix->channels;
+    // fixed tuning: the plan's MI shape, else 4 points per warp and 16 warps per CTA
+    Plan pl;
+    const void *kfn = nullptr;
+    if (cost == CGS_COST_MI) {
+        cgs_options od = o;
+        od.points_per_warp = 0;
+        od.warps_per_block = 0;
+        pl = choose_plan(cost, od, mi_bins);
+        kfn = kernel_mi(C, pl.G, pl.NW);
+    } else {
+        pl.G = 4;
+        pl.NW = 16;
+        kfn = loads_kernel_for(cost, C);
+    }
+    if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no allocation-free kernel for this cost / channel count");
+
+    DeviceInfo di;
+    if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+    const Staging st = staging_layout(*mov, *fix, 256, di.tex_pitch_align);
+    if (st.bytes > kStaticScratchBytes)
+        return fail(CGS_ERROR_INVALID_VALUE,
+                    "images too large for cgs_search_noalloc: staging needs " + std::to_string(st.bytes) +
+                        " bytes, the static scratch holds " + std::to_string(kStaticScratchBytes));
+    char *scratch = nullptr;
+    if ((s = static_scratch(di.dev, &scratch)) != CGS_SUCCESS) return s;
+
+    int32_t inc[8];
+    int64_t n64;
+    grid_increments(*grid, inc, &n64);
+    if (n64 > INT32_MAX) return fail(CGS_ERROR_GRID_TOO_LARGE, "grid has more than 2^31-1 points");
+    if (n64 <= 0) {
+        empty_result_kernel<<<1, 1, 0, stream>>>(result);
+        CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
+        return CGS_SUCCESS;
+    }
+
+    SearchParams p;
+    memset(&p, 0, sizeof(p));
+    for (int a = 0; a < 8; a++) {
+        p.start[a] = a < grid->dims ? grid->start[a] : 0.0f;
+        p.res[a] = a < grid->dims ? grid->resolution[a] : 0.0f;
+        p.inc[a] = inc[a];
+    }
+    p.dims = grid->dims;
+    p.n = (uint32_t)n64;
+    p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
+    p.exact_only = (o.flags & CGS_FLAG_EXACT_SAMPLES) ? 1 : 0;
+    if (!p.natural) {
+        locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
+        for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
+    }
+    if (cost_uses_theta(cost)) {
+        const int32_t n0 = grid->dims > 1 ? inc[1] : (int32_t)n64;
+        if (n0 > kMaxTrig) return fail(CGS_ERROR_UNSUPPORTED, "more than 256 values on the rotation axis");
+        for (int32_t i = 0; i < n0; i++) {
+            const float th = std::fmaf((float)i, grid->resolution[0], grid->start[0]);
+            p.trig[i] = make_float2(std::cos(th), std::sin(th));
+        }
+    }
+    p.mov_wf = (float)mov->width;
+    p.mov_hf = (float)mov->height;
+    p.cx = (float)mov->width / 2;
+    p.cy = (float)mov->height / 2;
+    p.mi_bins = mi_bins;
+    p.total_terms = (float)((double)fix->width * fix->height * C);
+    p.gate_n = (float)((double)o.overlap_gate * fix->width * fix->height * C);
+
+    const int64_t row_bytes = (int64_t)st.fpitch * 4 * C;
+    int R = (int)std::max<int64_t>(1, 16384 / row_bytes);
+    R = std::min(R, fix->height);
+    p.chunk_rows = R;
+    p.num_chunks = (fix->height + R - 1) / R;
+    const int64_t stage_bytes = (int64_t)R * row_bytes;
+    size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes + (size_t)pl.NW * pl.G * sizeof(ExactSlot);
+    if (cost == CGS_COST_MI) smem += (size_t)pl.NW * pl.G * (mi_bins + 1) * (mi_bins + 1) * 4;
+    else smem += (size_t)pl.NW * pl.G * accumulators(cost) * 32 * 4;
+    if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
+
+    // the static array is 256-byte aligned: the staging origin is its start
+    char *sb = scratch;
+    p.key = reinterpret_cast<unsigned long long *>(sb);
+    p.done = reinterpret_cast<unsigned int *>(sb + 8);
+    p.status = reinterpret_cast<unsigned int *>(sb + 12);
+    p.vmax = reinterpret_cast<float *>(sb + 16);
+    float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
+    float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
+    p.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};
+    p.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
+    p.costs = costs;
+    p.result = result;
+    p.mov_tex = 0;  // the plain-load kernels read no texture
+
+    PrepParams q;
+    q.mov_src = mov->data;
+    q.fix_src = fix->data;
+    q.mov_pix = mov->pixel;
+    q.fix_pix = fix->pixel;
+    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
+    q.mov_dst = mstage;
+    q.fix_dst = fstage;
+    q.mplane = st.mplane;
+    q.fplane = st.fplane;
+    q.mpitch = st.mpitch;
+    q.fpitch = st.fpitch;
+    q.key = p.key;
+    q.done = p.done;
+    q.status = p.status;
+    q.vmax = reinterpret_cast<float *>(sb + 16);
+    // the array keeps the previous call's contents: the header (argmin key, completion
+    // counter, status, max |pixel|) is cleared here and the staging kernel rewrites every
+    // staged element
+    cudaError_t e = cudaMemsetAsync(sb, 0, 256, stream);
+    if (e == cudaSuccess) {
+        const int64_t prep_elems = (st.mplane + st.fplane) * C;
+        prep_kernel<<<(int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8), 256, 0, stream>>>(q);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "prep_kernel");
+    const int threads = pl.NW * 32;
+    const uint32_t per_task = (uint32_t)(pl.NW * pl.G);
+    p.num_tasks = (p.n + per_task - 1) / per_task;
+    e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                   cudaSharedmemCarveoutMaxL1);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "search kernel setup");
+    if (per_sm < 1) return fail(CGS_ERROR_UNSUPPORTED, "search kernel does not fit on an SM");
+    const uint32_t blocks = std::min<uint32_t>(p.num_tasks, (uint32_t)(di.sms * per_sm));
+    void *args[] = {&p};
+    e = cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, smem, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "search kernel launch");
+    return CGS_SUCCESS;
+}
+
 cgs_status cgs_mi_histogram(const cgs_image *mov, const cgs_image *fix, const float params[8], int32_t bins,
                             uint32_t *hist, cgs_stream_t stream_) {
     cudaStream_t stream = (cudaStream_t)stream_;

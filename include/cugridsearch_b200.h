@@ -133,6 +133,26 @@ cgs_status cgs_search(const cgs_image *moving, const cgs_image *fixed, const cgs
  * with lowest-index ties.  result is a DEVICE pointer; params are left zero. */
 cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, cgs_stream_t stream);
 
+/* cgs_search without any device allocation.  This entry point has no counterpart in the
+ * reference; it exists for callers that cannot allocate device memory while they run: a
+ * real-time or streaming loop that reserves its memory budget up front, where an allocation
+ * may block on an implicit synchronisation or fail once a caching allocator (PyTorch's, for
+ * one) holds nearly all free memory, or a host that owns device memory through its own pool.
+ * Same arguments, results and status codes as cgs_search; the caller still provides the
+ * images, the costs array and the result.  Differences:
+ *   - scratch is a fixed 16 MiB array in the library's device image, held by every GPU that
+ *     loads the library until the process exits.  Images whose staged copies do not fit
+ *     (about 2 x 4 bytes x channels x width x height) are rejected with
+ *     CGS_ERROR_INVALID_VALUE and a message giving both sizes;
+ *   - the first call on a device looks up that array's device address (cudaGetSymbolAddress,
+ *     with the device current); make that first call before any stream capture;
+ *   - all calls on a device share the array, so calls that overlap on the GPU (on different
+ *     streams, or from different host threads) race: serialise them;
+ *   - points_per_warp / warps_per_block are ignored (4 points per warp, 16 warps; MI keeps its
+ *     own shape). */
+cgs_status cgs_search_noalloc(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
+                              const cgs_options *options, float *costs, cgs_argmin *result, cgs_stream_t stream);
+
 /* Joint histogram of the MI cost (CGS_COST_MI sampling: centred homography of params, the
  * calcNCC pixel loop) at one parameter vector: hist[bf * bins + bm] counts the (pixel, channel)
  * samples whose fixed value falls in bin bf and moving value in bin bm, bin = floor(v * bins / 256)
