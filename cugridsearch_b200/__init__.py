@@ -145,7 +145,7 @@ class CudaGrid:
 
 class CudaImage:
     """CudaImage<T, C> (include/cudaTensor.cuh:507-596) over a caller-owned CUDA tensor of
-    shape (H, W) or (H, W, C), dtype float32 or uint8, HWC row-major."""
+    shape (H, W) or (H, W, C), dtype float32, uint8, float64 or uint16, HWC row-major."""
 
     def __init__(self, tensor):
         torch = _torch()
@@ -155,12 +155,10 @@ class CudaImage:
             tensor = tensor.unsqueeze(-1)
         if tensor.dim() != 3 or not tensor.is_contiguous():
             raise ValueError("expected a contiguous (H, W) or (H, W, C) tensor")
-        if tensor.dtype == torch.float32:
-            pix = _abi.PIXEL_F32
-        elif tensor.dtype == torch.uint8:
-            pix = _abi.PIXEL_U8
-        else:
-            raise TypeError("pixel type must be float32 or uint8")
+        pix = {torch.float32: _abi.PIXEL_F32, torch.uint8: _abi.PIXEL_U8, torch.float64: _abi.PIXEL_F64,
+               torch.uint16: _abi.PIXEL_U16}.get(tensor.dtype)
+        if pix is None:
+            raise TypeError("pixel type must be float32, uint8, float64 or uint16")
         self.tensor = tensor
         h, w, c = tensor.shape
         self.img = CgsImage(tensor.data_ptr(), h, w, c, pix)

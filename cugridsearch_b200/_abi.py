@@ -16,7 +16,7 @@ COSTS = {
     "SAD_AVG": 0, "SAD_AVG_H": 1, "SAD_SUM_T": 2, "SAD_SUM_T_REF": 3, "SQD_REF": 4,
     "NCC_REF": 5, "SQD_ALT": 6, "NCC_ALT": 7, "MI_ALT": 8, "ZNCC": 9, "MI": 10,
 }
-PIXEL_F32, PIXEL_U8 = 0, 1
+PIXEL_F32, PIXEL_U8, PIXEL_F64, PIXEL_U16 = 0, 1, 2, 3
 FLAG_NATURAL_ORDER = 1
 FLAG_EXACT_SAMPLES = 2
 

@@ -207,7 +207,12 @@ struct PrepParams {
 };
 
 __device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
-    return pix == CGS_PIXEL_U8 ? (float)static_cast<const uint8_t *>(src)[i] : static_cast<const float *>(src)[i];
+    switch (pix) {
+        case CGS_PIXEL_U8: return (float)static_cast<const uint8_t *>(src)[i];
+        case CGS_PIXEL_F64: return (float)static_cast<const double *>(src)[i];  // rounded to nearest
+        case CGS_PIXEL_U16: return (float)static_cast<const uint16_t *>(src)[i];
+        default: return static_cast<const float *>(src)[i];
+    }
 }
 
 // HWC images -> one zero-padded FP32 plane per channel.  Moving planes are (H + 1) rows of
@@ -440,7 +445,7 @@ static cgs_status check_image(const cgs_image *im, const char *name) {
     if (!im->data) return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + "->data is null");
     if (im->height < 1 || im->width < 1)
         return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " has an empty size");
-    if (im->pixel != CGS_PIXEL_F32 && im->pixel != CGS_PIXEL_U8)
+    if (im->pixel < CGS_PIXEL_F32 || im->pixel > CGS_PIXEL_U16)
         return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " has an unknown pixel type");
     if (im->channels < 1 || im->channels > 4)
         return fail(CGS_ERROR_INVALID_VALUE, std::string(name) + " must have 1..4 channels");

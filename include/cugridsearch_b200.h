@@ -51,7 +51,9 @@ typedef enum cgs_cost {
     CGS_COST_COUNT = 11
 } cgs_cost;
 
-typedef enum cgs_pixel { CGS_PIXEL_F32 = 0, CGS_PIXEL_U8 = 1 } cgs_pixel;
+/* Pixel types of CudaImage<T, C>.  Every tap is converted to float as the reference's
+ * valueAt_bilinear does (float tlc = _data[...], include/cudaTensor.cuh:563). */
+typedef enum cgs_pixel { CGS_PIXEL_F32 = 0, CGS_PIXEL_U8 = 1, CGS_PIXEL_F64 = 2, CGS_PIXEL_U16 = 3 } cgs_pixel;
 
 /* CudaImage<T, C> (include/cudaTensor.cuh:507-596): dims {C, W, H}, HWC row-major,
  * element (y, x, c) at c + C * (x + W * y).  data is a caller-owned DEVICE pointer. */

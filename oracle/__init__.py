@@ -31,7 +31,7 @@ COSTS = {
     "SAD_AVG": 0, "SAD_AVG_H": 1, "SAD_SUM_T": 2, "SAD_SUM_T_REF": 3, "SQD_REF": 4,
     "NCC_REF": 5, "SQD_ALT": 6, "NCC_ALT": 7, "MI_ALT": 8, "ZNCC": 9, "MI": 10,
 }
-PIX = {np.dtype(np.float32): 0, np.dtype(np.uint8): 1}
+PIX = {np.dtype(np.float32): 0, np.dtype(np.uint8): 1, np.dtype(np.float64): 2, np.dtype(np.uint16): 3}
 
 _lock = threading.Lock()
 _lib = None

@@ -30,8 +30,12 @@
 static inline float og_at(const og_image *im, int64_t flat) {
     int64_t total = (int64_t)im->height * im->width * im->channels;
     if (flat < 0 || flat >= total) return 0.0f; /* past-the-end read: zero pad */
-    if (im->pix == OG_PIX_U8) return (float)((const uint8_t *)im->data)[flat];
-    return ((const float *)im->data)[flat];
+    switch (im->pix) {
+        case OG_PIX_U8: return (float)((const uint8_t *)im->data)[flat];
+        case OG_PIX_F64: return (float)((const double *)im->data)[flat];
+        case OG_PIX_U16: return (float)((const uint16_t *)im->data)[flat];
+        default: return ((const float *)im->data)[flat];
+    }
 }
 
 /* CudaImage::inImage (cudaTensor.cuh:548-550): float coordinates against int sizes. */

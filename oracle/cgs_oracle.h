@@ -35,12 +35,12 @@ enum {
     OG_NUM_COSTS = 11
 };
 
-enum { OG_PIX_F32 = 0, OG_PIX_U8 = 1 };
+enum { OG_PIX_F32 = 0, OG_PIX_U8 = 1, OG_PIX_F64 = 2, OG_PIX_U16 = 3 };
 
 typedef struct {
     const void *data;   /* host pointer, HWC row-major (CudaImage layout, cudaTensor.cuh:512-534) */
     int32_t height, width, channels;
-    int32_t pix;        /* OG_PIX_F32 or OG_PIX_U8 */
+    int32_t pix;        /* OG_PIX_* */
 } og_image;
 
 /* Options for the costs that have no reference counterpart. */

@@ -77,11 +77,15 @@ float eval_p(int cost, const float *params, const void *mov, int mh, int mw, con
 
 extern "C" {
 
-/* One reference functor evaluation. pix: 0 = float, 1 = uint8_t. */
+/* One reference functor evaluation. pix: 0 = float, 1 = uint8_t, 2 = double, 3 = uint16_t. */
 float cgsref_eval(int cost, const float *params, int pix, const void *mov, int mh, int mw, const void *fix, int fh,
                   int fw, int channels) {
-    if (pix == 1) return eval_p<uint8_t>(cost, params, mov, mh, mw, fix, fh, fw, channels);
-    return eval_p<float>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+    switch (pix) {
+        case 1: return eval_p<uint8_t>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+        case 2: return eval_p<double>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+        case 3: return eval_p<uint16_t>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+        default: return eval_p<float>(cost, params, mov, mh, mw, fix, fh, fw, channels);
+    }
 }
 
 /* The reference's homography helpers, for bit-exact tests of the oracle restatement. */
