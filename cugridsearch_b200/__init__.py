@@ -197,19 +197,24 @@ class CudaTensor:
 
 
 def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0,
-             warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool = False) -> CgsOptions:
+             warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool | None = None) -> CgsOptions:
     if cost not in COSTS:
         raise ValueError(f"unknown cost {cost!r}")
-    flags = (_abi.FLAG_NATURAL_ORDER if natural_order else 0) | (_abi.FLAG_EXACT_SAMPLES if exact_samples else 0)
+    flags = _abi.FLAG_NATURAL_ORDER if natural_order else 0
+    if exact_samples is True:
+        flags |= _abi.FLAG_EXACT_SAMPLES
+    elif exact_samples is False:
+        flags |= _abi.FLAG_FAST_SAMPLES
     return CgsOptions(COSTS[cost], mi_bins, overlap_gate, points_per_warp, warps_per_block, flags)
 
 
 def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs=None, stream=None,
            mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0, warps_per_block: int = 0,
-           natural_order: bool = False, exact_samples: bool = False, result=None) -> Argmin | None:
+           natural_order: bool = False, exact_samples: bool | None = None, result=None) -> Argmin | None:
     """Run one fused search.  With ``result`` (a CUDA uint8 tensor of sizeof(cgs_argmin)
     bytes) the call is asynchronous and returns None; otherwise it synchronises and
-    returns the :class:`Argmin`."""
+    returns the :class:`Argmin`.  ``exact_samples``: None = the cost's default (exact for
+    the reference functors, fast for ZNCC / MI), True / False force a mode."""
     opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples)
     cptr = costs.data_ptr() if costs is not None else None
     s = _stream_handle(stream)

@@ -19,6 +19,7 @@ COSTS = {
 PIXEL_F32, PIXEL_U8, PIXEL_F64, PIXEL_U16 = 0, 1, 2, 3
 FLAG_NATURAL_ORDER = 1
 FLAG_EXACT_SAMPLES = 2
+FLAG_FAST_SAMPLES = 4
 
 STATUS = {
     0: "CGS_SUCCESS", 1: "CGS_ERROR_INVALID_VALUE", 2: "CGS_ERROR_UNSUPPORTED",

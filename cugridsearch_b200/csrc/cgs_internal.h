@@ -16,6 +16,10 @@ const void *kernel_ncc_ref(int C, int G, int NW);
 const void *kernel_zncc(int C, int G, int NW);
 const void *kernel_mi(int C, int G, int NW);
 
+// Scanline functors (calcSQDAlt, calcNCCAlt, calcMIAlt) and their shared-memory size.
+const void *kernel_scan(int cost, int C);
+size_t scan_smem_bytes(int cost);
+
 // Plain-load (no texture object) variants at 4 points per warp and 16 warps, for the
 // allocation-free entry point.
 const void *kernel_sad_avg_loads(int C);

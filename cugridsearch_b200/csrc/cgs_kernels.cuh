@@ -58,6 +58,8 @@ struct SearchParams {
     unsigned int *status;
     const float *vmax;   // max |moving pixel| (from the staging kernel)
     cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
+    const float *row_table;       // calcMIAlt's row values (the float recurrence row += 1/(H_f-1))
+    int32_t n_rows;
     cgs_argmin *result;
     // cost options
     int32_t mi_bins;
@@ -114,10 +116,15 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
-// Fast-path state of one grid point (registers).
+// Fast-path state of one grid point (registers).  The per-row terms (B, P - Q, C2, R - S,
+// D2, T - U) live in shared memory and are read once per row.
 struct FastMap {
-    float A, B, PQ, C1, C2, RS, D1, D2, TU;  // PQ = P - Q etc.
-    float li_x, lo_x, li_y, lo_y;           // |m - half| < li: clearly inside; > lo: clearly outside
+    float A, C1, D1;
+    float li_x, lo_x, li_y, lo_y;  // |m - half| < li: clearly inside; > lo: clearly outside
+};
+
+struct RowTerms {
+    float B, PQ, C2, RS, D2, TU;
 };
 
 // Error bound of the fast coordinates against the exact ones, over the whole fixed image.
@@ -132,11 +139,12 @@ struct FastMap {
 // 7.2u M_w / w_lo + 4.1u, which must stay small for "clearly outside" to hold there.  A
 // point whose w may change sign over the image, or whose bound is not small, takes the
 // exact path everywhere.
-__device__ __forceinline__ void map_guard(const MapCoef &k, const SearchParams &p, FastMap &f, float &gx_out,
-                                          float &gy_out) {
-    f.A = k.A; f.B = k.B; f.PQ = k.P - k.Q;
-    f.C1 = k.C1; f.C2 = k.C2; f.RS = k.R - k.S;
-    f.D1 = k.D1; f.D2 = k.D2; f.TU = k.T - k.U;
+__device__ __forceinline__ void map_guard(const MapCoef &k, const SearchParams &p, FastMap &f, RowTerms &rt,
+                                          float &gx_out, float &gy_out) {
+    f.A = k.A;
+    f.C1 = k.C1;
+    f.D1 = k.D1;
+    rt = RowTerms{k.B, k.P - k.Q, k.C2, k.R - k.S, k.D2, k.T - k.U};
     const double u = 5.9604644775390625e-8;  // 2^-24
     const double X1 = (double)p.fix.w - 1.0, Y1 = (double)p.fix.h - 1.0;
     const double A = k.A, B = k.B, PQ = (double)k.P - (double)k.Q;
@@ -344,9 +352,11 @@ struct MiGuard {
     float sgx, sgy, hx, hy;
 };
 
-// Shared-memory copy of a grid point's exact-path coefficients and guards.
+// Shared-memory copy of a grid point's exact-path coefficients, guards and row terms.
 struct ExactSlot {
     float P, Q, R, S, T, U, gx, gy;
+    RowTerms rt;
+    float B, C2, D2, pad;
 };
 
 // NW warps per CTA; 512 / (32 NW) CTAs share an SM (two CTAs of 8 warps hide each
@@ -441,12 +451,13 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
             const float2 cs = p.trig[min(ax[0], kMaxTrig - 1)];
             const MapCoef kc = make_coef<COST>(q, cs, p);
             float gx, gy;
-            map_guard(kc, p, fm[g], gx, gy);
+            RowTerms rt;
+            map_guard(kc, p, fm[g], rt, gx, gy);
             mg[g].sgx = sB * gx;
             mg[g].sgy = sB * gy;
             mg[g].hx = 0.5f - gx;
             mg[g].hy = 0.5f - gy;
-            if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy};
+            if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy, rt, kc.B, kc.C2, kc.D2, 0.0f};
         }
 
         float *tot = totals + warp * G * NA * 32 + lane;
@@ -487,9 +498,10 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                 const float yf = (float)(r0 + yrow);
 #pragma unroll
                 for (int g = 0; g < G; g++) {
-                    byw[g] = fmaf(fm[g].B, yf, fm[g].PQ);
-                    byx[g] = fmaf(fm[g].C2, yf, fm[g].RS);
-                    byy[g] = fmaf(fm[g].D2, yf, fm[g].TU);
+                    const RowTerms rt = my_slots[g].rt;
+                    byw[g] = fmaf(rt.B, yf, rt.PQ);
+                    byx[g] = fmaf(rt.C2, yf, rt.RS);
+                    byy[g] = fmaf(rt.D2, yf, rt.TU);
                 }
             };
             set_row(yy);
@@ -565,8 +577,8 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                     for (int g = 0; g < G; g++) {
                         if (amb[g]) {
                             const ExactSlot &sl = my_slots[g];
-                            const MapCoef kc{fm[g].A, fm[g].B, sl.P, sl.Q, fm[g].C1, fm[g].C2, sl.R, sl.S,
-                                             fm[g].D1, fm[g].D2, sl.T, sl.U};
+                            const MapCoef kc{fm[g].A, sl.B, sl.P, sl.Q, fm[g].C1, sl.C2, sl.R, sl.S,
+                                             fm[g].D1, sl.D2, sl.T, sl.U};
                             float ex, ey;
                             exact_map(kc, xf, (float)(r0 + yy), ex, ey);
                             if (in_image(ey, ex, p.mov_wf, p.mov_hf)) {

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "cgs_internal.h"
+#include "cgs_scan.cuh"
 
 namespace cgs {
 
@@ -204,6 +205,9 @@ struct PrepParams {
     unsigned int *done;
     unsigned int *status;
     float *vmax;  // zeroed before the launch
+    int32_t fix_alias;   // stage the fixed image like the moving one (scanline functors)
+    float *row_table;    // calcMIAlt row values, or null
+    int32_t rowsf;
 };
 
 __device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
@@ -250,7 +254,20 @@ __global__ void prep_kernel(const PrepParams q) {
         const int64_t y = e / q.fpitch, x = e - y * q.fpitch;
         float v = 0.0f;
         if (y < q.fh && x < q.fw) v = load_pix(q.fix_src, q.fix_pix, (y * q.fw + x) * q.c + c);
+        else if (q.fix_alias && y + 1 < q.fh && x == q.fw)
+            v = load_pix(q.fix_src, q.fix_pix, ((y + 1) * q.fw) * q.c + c);
         q.fix_dst[i] = v;
+    }
+    if (q.row_table && tid == 0) {
+        // calcMIAlt's rows: row = -0.5; while (row < 0.5) row += 1 / (float)(rowsf - 1)
+        // (cudaErrorFunction_mi.cuh:164), the same float additions as the reference
+        float row = -0.5f;
+        int n = 0;
+        const float inc = 1.0f / (float)(q.rowsf - 1);
+        while ((double)row < 0.5 && n < q.rowsf + 2) {
+            q.row_table[n++] = row;
+            row = __fadd_rn(row, inc);
+        }
     }
 }
 
@@ -348,20 +365,45 @@ static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 struct Staging {
     int32_t mpitch = 0, fpitch = 0;
     int64_t mplane = 0, fplane = 0;
-    size_t mov_off = 0, fix_off = 0, bytes = 0;
+    size_t mov_off = 0, fix_off = 0, rows_off = 0, bytes = 0;
 };
 
-static Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align) {
+// Sampling mode of a request (see CGS_FLAG_EXACT_SAMPLES / CGS_FLAG_FAST_SAMPLES).
+static bool exact_samples(int cost, int flags) {
+    if (flags & CGS_FLAG_EXACT_SAMPLES) return true;
+    if (flags & CGS_FLAG_FAST_SAMPLES) return false;
+    return !(cost == CGS_COST_ZNCC || cost == CGS_COST_MI);
+}
+
+static bool is_scanline(int cost) {
+    return cost == CGS_COST_SQD_ALT || cost == CGS_COST_NCC_ALT || cost == CGS_COST_MI_ALT;
+}
+
+// Number of rows calcMIAlt visits (the float recurrence of its row loop, on the host).
+static int32_t mi_alt_rows(int rowsf) {
+    float row = -0.5f;
+    int n = 0;
+    const float inc = 1.0f / (float)(rowsf - 1);
+    while ((double)row < 0.5 && n < rowsf + 2) {
+        n++;
+        row = row + inc;
+    }
+    return n;
+}
+
+static Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align,
+                              bool fix_alias = false, bool row_table = false) {
     Staging st;
     const int C = fix.channels;
     st.mpitch = (int32_t)round_up(mov.width + 1, std::max(1, tex_pitch_align / 4));
     st.mplane = (int64_t)(mov.height + 1) * st.mpitch;
-    st.fpitch = (int32_t)round_up(fix.width, 4);
-    st.fplane = round_up((int64_t)fix.height * st.fpitch, 64);
+    st.fpitch = (int32_t)round_up(fix.width + (fix_alias ? 1 : 0), 4);
+    st.fplane = round_up((int64_t)(fix.height + (fix_alias ? 1 : 0)) * st.fpitch, 64);
     // offsets from a tex_align-aligned origin; the allocation carries tex_align bytes of slack
     st.mov_off = (size_t)round_up(256, tex_align);
     st.fix_off = st.mov_off + (size_t)round_up(st.mplane * C * 4, 256);
-    st.bytes = st.fix_off + (size_t)st.fplane * C * 4 + (size_t)tex_align;
+    st.rows_off = st.fix_off + (size_t)round_up(st.fplane * C * 4, 256);
+    st.bytes = st.rows_off + (row_table ? (size_t)round_up((int64_t)(fix.height + 2) * 4, 256) : 0) + (size_t)tex_align;
     return st;
 }
 
@@ -496,6 +538,114 @@ static Plan choose_plan(int cost, const cgs_options &o, int mi_bins) {
     return pl;
 }
 
+// The scanline functors: staging with both images aliased, the calcMIAlt row table, one warp
+// per grid point.  Arguments are validated by cgs_search.
+static cgs_status search_scanline(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid,
+                                  const cgs_options &o, float *costs, cgs_argmin *result, cudaStream_t stream,
+                                  const DeviceInfo &di) {
+    const int cost = o.cost;
+    const int C = fix->channels;
+    const void *kfn = kernel_scan(cost, C);
+    if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no scanline kernel for this channel count");
+    int32_t inc[8];
+    int64_t n64;
+    grid_increments(*grid, inc, &n64);
+    if (n64 > INT32_MAX) return fail(CGS_ERROR_GRID_TOO_LARGE, "grid has more than 2^31-1 points");
+    if (n64 <= 0) {
+        empty_result_kernel<<<1, 1, 0, stream>>>(result);
+        CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
+        return CGS_SUCCESS;
+    }
+    SearchParams p;
+    memset(&p, 0, sizeof(p));
+    for (int a = 0; a < 8; a++) {
+        p.start[a] = a < grid->dims ? grid->start[a] : 0.0f;
+        p.res[a] = a < grid->dims ? grid->resolution[a] : 0.0f;
+        p.inc[a] = inc[a];
+    }
+    p.dims = grid->dims;
+    p.n = (uint32_t)n64;
+    p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
+    if (!p.natural) {
+        locality_order(cost == CGS_COST_MI_ALT ? CGS_COST_SAD_AVG : cost, *grid, fix->width, fix->height, mov->width,
+                       mov->height, p.perm);
+        for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
+    }
+    const int32_t n0 = grid->dims > 1 ? inc[1] : (int32_t)n64;
+    if (n0 > kMaxTrig) return fail(CGS_ERROR_UNSUPPORTED, "more than 256 values on the rotation axis");
+    for (int32_t i = 0; i < n0; i++) {
+        const float th = std::fmaf((float)i, grid->resolution[0], grid->start[0]);
+        p.trig[i] = make_float2(std::cos(th), std::sin(th));
+    }
+    p.mov_wf = (float)mov->width;
+    p.mov_hf = (float)mov->height;
+    p.cx = (float)mov->width / 2;
+    p.cy = (float)mov->height / 2;
+    const bool mi = cost == CGS_COST_MI_ALT;
+    p.n_rows = mi ? mi_alt_rows(fix->height) : fix->height;
+
+    const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align, true, mi);
+    cgs_status s;
+    cudaMemPool_t pool;
+    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
+    void *scratch = nullptr;
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes, pool, stream), "cudaMallocFromPoolAsync");
+    char *sb = staging_origin(scratch, di.tex_align);
+    p.key = reinterpret_cast<unsigned long long *>(sb);
+    p.done = reinterpret_cast<unsigned int *>(sb + 8);
+    p.status = reinterpret_cast<unsigned int *>(sb + 12);
+    p.vmax = reinterpret_cast<float *>(sb + 16);
+    float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
+    float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
+    float *rtab = mi ? reinterpret_cast<float *>(sb + st.rows_off) : nullptr;
+    p.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};
+    p.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
+    p.row_table = rtab;
+    p.costs = costs;
+    p.result = result;
+
+    PrepParams q{};  // every field zero unless set below
+
+    q.mov_src = mov->data;
+    q.fix_src = fix->data;
+    q.mov_pix = mov->pixel;
+    q.fix_pix = fix->pixel;
+    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
+    q.mov_dst = mstage;
+    q.fix_dst = fstage;
+    q.mplane = st.mplane;
+    q.fplane = st.fplane;
+    q.mpitch = st.mpitch;
+    q.fpitch = st.fpitch;
+    q.key = p.key;
+    q.done = p.done;
+    q.status = p.status;
+    q.vmax = reinterpret_cast<float *>(sb + 16);
+    q.fix_alias = 1;
+    q.row_table = rtab;
+    q.rowsf = fix->height;
+    cudaError_t e = cudaMemsetAsync(sb, 0, 256, stream);
+    if (e == cudaSuccess) {
+        const int64_t prep_elems = (st.mplane + st.fplane) * C;
+        prep_kernel<<<(int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8), 256, 0, stream>>>(q);
+        e = cudaGetLastError();
+    }
+    const size_t smem = scan_smem_bytes(cost);
+    const int threads = kScanWarps * 32;
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+    if (e == cudaSuccess && per_sm >= 1) {
+        const uint32_t blocks = std::min<uint32_t>((p.n + kScanWarps - 1) / kScanWarps, (uint32_t)(di.sms * per_sm));
+        void *args[] = {&p};
+        e = cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, smem, stream);
+    }
+    cudaFreeAsync(scratch, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "scanline kernel");
+    if (per_sm < 1) return fail(CGS_ERROR_UNSUPPORTED, "scanline kernel does not fit on an SM");
+    return CGS_SUCCESS;
+}
+
 }  // namespace cgs
 
 using namespace cgs;
@@ -600,6 +750,11 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
         if (mi_bins < 2 || mi_bins > 64 || (mi_bins & (mi_bins - 1)))
             return fail(CGS_ERROR_INVALID_VALUE, "mi_bins must be a power of two in [2, 64]");
     }
+    if (is_scanline(cost)) {
+        DeviceInfo dsi;
+        if ((s = device_info(&dsi)) != CGS_SUCCESS) return s;
+        return search_scanline(mov, fix, grid, o, costs, result, stream, dsi);
+    }
     KernelGetter getter = getter_for(cost);
     if (!getter) return fail(CGS_ERROR_UNSUPPORTED, "cost not implemented by this build");
     const int C = fix->channels;
@@ -630,7 +785,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.dims = grid->dims;
     p.n = (uint32_t)n64;
     p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
-    p.exact_only = (o.flags & CGS_FLAG_EXACT_SAMPLES) ? 1 : 0;
+    p.exact_only = exact_samples(cost, o.flags) ? 1 : 0;
     if (!p.natural) {
         locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
         for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
@@ -681,7 +836,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.costs = costs;
     p.result = result;
 
-    PrepParams q;
+    PrepParams q{};  // every field zero unless set below
     q.mov_src = mov->data;
     q.fix_src = fix->data;
     q.mov_pix = mov->pixel;
@@ -891,7 +1046,7 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
     p.dims = grid->dims;
     p.n = (uint32_t)n64;
     p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
-    p.exact_only = (o.flags & CGS_FLAG_EXACT_SAMPLES) ? 1 : 0;
+    p.exact_only = exact_samples(cost, o.flags) ? 1 : 0;
     if (!p.natural) {
         locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
         for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
@@ -937,7 +1092,7 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
     p.result = result;
     p.mov_tex = 0;  // the plain-load kernels read no texture
 
-    PrepParams q;
+    PrepParams q{};  // every field zero unless set below
     q.mov_src = mov->data;
     q.fix_src = fix->data;
     q.mov_pix = mov->pixel;
@@ -1001,7 +1156,7 @@ cgs_status cgs_mi_histogram(const cgs_image *mov, const cgs_image *fix, const fl
     char *sb = staging_origin(scratch, di.tex_align);
     float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
     float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
-    PrepParams q;
+    PrepParams q{};  // every field zero unless set below
     q.mov_src = mov->data; q.fix_src = fix->data; q.mov_pix = mov->pixel; q.fix_pix = fix->pixel;
     q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
     q.mov_dst = mstage; q.fix_dst = fstage; q.mplane = st.mplane; q.fplane = st.fplane;
@@ -1018,7 +1173,7 @@ cgs_status cgs_mi_histogram(const cgs_image *mov, const cgs_image *fix, const fl
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
-        HistParams hp;
+        HistParams hp{};
         hp.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};
         hp.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
         hp.mov_wf = (float)mov->width;

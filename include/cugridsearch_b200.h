@@ -88,9 +88,14 @@ typedef struct cgs_options {
 /* Evaluate grid points in the reference's index order (axis 0 fastest) instead of the
  * locality order the library picks.  Results are identical; only speed differs. */
 #define CGS_FLAG_NATURAL_ORDER 1
-/* Take every sample through the reference's exact operation sequence (the kernel otherwise
- * does so only where a decision is close: see the kernel notes).  For verification. */
+/* Sampling modes.  Every mode makes the reference's discrete decisions exactly (which
+ * samples fall inside the moving image; MI bins).  EXACT additionally forms every sample
+ * with the reference's operation sequence, so sample values are bit-identical to the
+ * reference's host path; FAST forms them with fused arithmetic (FP32-accurate, about 1e-6
+ * relative) and is about twice as fast.  Default: EXACT for the reference functors (costs
+ * 0-8), FAST for CGS_COST_ZNCC and CGS_COST_MI.  The scanline functors (6-8) are always exact. */
 #define CGS_FLAG_EXACT_SAMPLES 2
+#define CGS_FLAG_FAST_SAMPLES 4
 
 /* Argmin of a search: the lowest cost, ties broken by the lowest grid index.  NaN and
  * +inf costs never win (the reference compares with '<', cudaTensor.cuh:256 and

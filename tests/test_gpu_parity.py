@@ -58,22 +58,29 @@ def _check(res, costs, c32, c64, cost, grid):
     np.testing.assert_array_equal(res.params[: grid.getDimension()], grid.getGridPoint(res.index))
 
 
-EIGHT_PARAM = ["SAD_AVG", "SQD_REF", "NCC_REF", "ZNCC", "MI"]
+EIGHT_PARAM = ["SAD_AVG", "SQD_REF", "NCC_REF", "ZNCC", "MI", "SQD_ALT", "NCC_ALT", "MI_ALT"]
+
+
+def _pair(seed, size, cost, **kw):
+    p = S.small_pair(seed, size=size, count=3, cost=cost, **kw)
+    if cost == "MI_ALT":  # calcMIAlt's translations are fractions of the image
+        p.lo[4:6], p.hi[4:6] = -0.15, 0.15
+    return p
 
 
 @pytest.mark.parametrize("u8", [False, True])
 @pytest.mark.parametrize("cost", EIGHT_PARAM)
 def test_eight_param_costs_match_oracle(cuda, lib, cost, u8):
-    pair = S.small_pair(101, size=32, count=3, cost=cost, u8=u8)
+    pair = _pair(101, 32, cost, u8=u8)
     res, costs, grid = _gpu_search(cuda, pair, cost)
     c32, c64 = _oracle(pair, cost)
     _check(res, costs, c32, c64, cost, grid)
 
 
-@pytest.mark.parametrize("cost", ["SAD_AVG", "NCC_REF", "ZNCC", "MI", "SQD_REF"])
+@pytest.mark.parametrize("cost", ["SAD_AVG", "NCC_REF", "ZNCC", "MI", "SQD_REF", "SQD_ALT", "NCC_ALT", "MI_ALT"])
 def test_ragged_sizes_and_channels(cuda, lib, cost):
     # fixed 29 wide, moving 23 wide: odd row pitches, the W-1 < x < W alias, last-row pad
-    pair = S.small_pair(7, size=29, count=3, cost=cost, msize=23, channels=3)
+    pair = _pair(7, 29, cost, msize=23, channels=3)
     res, costs, grid = _gpu_search(cuda, pair, cost)
     c32, c64 = _oracle(pair, cost)
     _check(res, costs, c32, c64, cost, grid)
@@ -177,14 +184,14 @@ def test_mi_histogram_counts_exact(cuda, lib, u8, bins):
 
 @pytest.mark.parametrize("cost", ["MI", "SAD_AVG", "NCC_REF", "ZNCC", "SQD_REF", "SAD_AVG_H"])
 def test_fast_path_decisions_match_exact_path(cuda, lib, cost):
-    """The guarded fast path makes the same decisions as the all-exact path: MI costs are
-    bit-identical (identical histograms), other costs agree to rounding."""
+    """The guarded fast sampling mode makes the same decisions as the exact mode: MI costs are
+    bit-identical (identical histograms), other costs agree to rounding on smooth images."""
     pair = S.small_pair(29, size=96, count=3, cost=cost, u8=(cost == "MI"))
     dg = None
     if cost == "SAD_AVG_H":
         dg = ([0.95, -0.05, -4.0, -0.05, 0.95, -4.0, -1e-4, -1e-4], [1.05, 0.05, 4.0, 0.05, 1.05, 4.0, 1e-4, 1e-4],
               [3] * 8)
-    rf, cf, _ = _gpu_search(cuda, pair, cost, dims_grid=dg)
+    rf, cf, _ = _gpu_search(cuda, pair, cost, dims_grid=dg, exact_samples=False)
     re, ce, _ = _gpu_search(cuda, pair, cost, dims_grid=dg, exact_samples=True)
     if cost == "MI":
         np.testing.assert_array_equal(cf, ce)
