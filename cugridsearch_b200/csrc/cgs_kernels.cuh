@@ -490,6 +490,95 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
 #pragma unroll
                 for (int j = 0; j < NA; j++) part[g][j] = 0.0f;
 
+            if (p.exact_only) {
+                // Exact sampling: coordinates, tap weights and values in the reference's
+                // operation order (calcNewCoordH + valueAt_bilinear), so every sample is the
+                // reference's bit for bit.  Row products B*y, C2*y, D2*y are formed once per row.
+                float ek[G][9];  // A, C1, D1, P, Q, R, S, T, U
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const ExactSlot &sl = my_slots[g];
+                    ek[g][0] = fm[g].A; ek[g][1] = fm[g].C1; ek[g][2] = fm[g].D1;
+                    ek[g][3] = sl.P; ek[g][4] = sl.Q; ek[g][5] = sl.R; ek[g][6] = sl.S; ek[g][7] = sl.T; ek[g][8] = sl.U;
+                }
+                int xx = lane, yy = 0;
+                while (xx >= fw) { xx -= fw; yy++; }
+                float xf = (float)xx;
+                float eb[G][3];
+                auto set_row_e = [&](int yrow) {
+                    const float yf = (float)(r0 + yrow);
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const ExactSlot &sl = my_slots[g];
+                        eb[g][0] = xm(sl.B, yf);
+                        eb[g][1] = xm(sl.C2, yf);
+                        eb[g][2] = xm(sl.D2, yf);
+                    }
+                };
+                set_row_e(yy);
+                while (yy < rows) {
+                    FixTerms ft[C];
+#pragma unroll
+                    for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], p);
+                    float ex[G], ey[G];
+                    bool ins[G];
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const float w = xs(xa(xa(xm(ek[g][0], xf), eb[g][0]), ek[g][3]), ek[g][4]);
+                        const float X = xs(xa(xa(xm(ek[g][1], xf), eb[g][1]), ek[g][5]), ek[g][6]);
+                        const float Y = xs(xa(xa(xm(ek[g][2], xf), eb[g][2]), ek[g][7]), ek[g][8]);
+                        ex[g] = xd(X, w);
+                        ey[g] = xd(Y, w);
+                        ins[g] = in_image(ey[g], ex[g], p.mov_wf, p.mov_hf);
+                    }
+                    float v[G][C];
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const float fx = ins[g] ? floorf(ex[g]) : 0.0f, fy = ins[g] ? floorf(ey[g]) : 0.0f;
+                        const float ax = xs(ex[g], fx), ay = xs(ey[g], fy);
+                        const float omx = xs(1.0f, ax), omy = xs(1.0f, ay);
+                        const float u = ins[g] ? fx + 1.0f : -4.0f;
+                        const int base = (int)fx + mpitch * (int)fy;
+#pragma unroll
+                        for (int c = 0; c < C; c++) {
+                            float v00, v01, v10, v11;
+                            if constexpr (kTexTaps) {
+                                const float4 t4 = tex2Dgather<float4>(p.mov_tex, u, fy + 1.0f + (float)c * mrows, 0);
+                                v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
+                            } else {
+                                const float *pl = mdata + c * mplane + base;
+                                v00 = __ldg(pl); v01 = __ldg(pl + 1);
+                                v10 = __ldg(pl + mpitch); v11 = __ldg(pl + mpitch + 1);
+                            }
+                            const float top = xa(xm(omx, v00), xm(ax, v01));
+                            const float bot = xa(xm(omx, v10), xm(ax, v11));
+                            v[g][c] = ins[g] ? xa(xm(omy, top), xm(ay, bot)) : 0.0f;
+                        }
+                    }
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        if (ins[g] || kAllPixels) {
+#pragma unroll
+                            for (int c = 0; c < C; c++) {
+                                if constexpr (kMI) {
+                                    const int bm = min(max((int)floorf(v[g][c] * sB), 0), B - 1);
+                                    atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
+                                } else {
+                                    accumulate<COST>(part[g], ft[c], v[g][c]);
+                                }
+                            }
+                            cnt[g] += C;
+                        }
+                    }
+                    xx += 32;
+                    xf += 32.0f;
+                    if (xx >= fw) {
+                        do { xx -= fw; yy++; } while (xx >= fw);
+                        xf = (float)xx;
+                        if (yy < rows) set_row_e(yy);
+                    }
+                }
+            } else {
             int xx = lane, yy = 0;
             while (xx >= fw) { xx -= fw; yy++; }
             float xf = (float)xx;
@@ -617,6 +706,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                     if (yy < rows) set_row(yy);
                 }
             }
+            }  // fast sampling
             if constexpr (!kMI) {
 #pragma unroll
                 for (int g = 0; g < G; g++)
