@@ -246,6 +246,17 @@ def mi_histogram(moving: CudaImage, fixed: CudaImage, params, bins: int = 32, st
     return h.cpu().numpy().view(np.uint32).reshape(bins, bins)
 
 
+def covariance(grid: CudaGrid, costs, stream=None) -> np.ndarray:
+    """CudaGridSearcher::covariance_by_value on a cost tensor (cgs_covariance): the
+    dims x dims curvature matrix around the grid minimum, summed in double."""
+    torch = _torch()
+    d = grid.g.dims
+    out = torch.empty(d * d, dtype=torch.float64, device=costs.device)
+    check(_abi.load().cgs_covariance(C.byref(grid.g), costs.data_ptr(), costs.numel(), out.data_ptr(),
+                                     _stream_handle(stream)))
+    return out.cpu().numpy().reshape(d, d)
+
+
 def result_buffer(device=None):
     """A device buffer for one asynchronous cgs_argmin result."""
     torch = _torch()
@@ -293,3 +304,15 @@ class CudaGridSearcher:
 
     def search_by_reference_stream(self, fn, STREAM_BLOCK_DIM, numCores, moving, fixed, **kw):
         return self._run(fn, moving, fixed, **kw)
+
+    def covariance_by_value(self, covar_matrix=None) -> np.ndarray:
+        """Curvature matrix around the minimum of the result tensor (D x D); added into
+        covar_matrix when one is given, as the reference adds into its buffer."""
+        if self._result is None:
+            raise ValueError("covariance_by_value needs the result tensor")
+        n = self._grid.numElements()
+        cov = covariance(self._grid, self._result.tensor.reshape(-1)[:n])
+        if covar_matrix is not None:
+            covar_matrix += cov.astype(covar_matrix.dtype).reshape(covar_matrix.shape)
+            return covar_matrix
+        return cov

@@ -31,7 +31,7 @@ STATUS = {
 EXPORTS = [
     "cgs_grid_update", "cgs_grid_num_elements", "cgs_grid_point", "cgs_search",
     "cgs_argmin_f32", "cgs_search_sync", "cgs_status_string", "cgs_last_error", "cgs_version",
-    "cgs_mi_histogram", "cgs_search_noalloc",
+    "cgs_mi_histogram", "cgs_search_noalloc", "cgs_covariance",
 ]
 
 
@@ -94,6 +94,8 @@ def load() -> C.CDLL:
         L.cgs_argmin_f32.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
         L.cgs_mi_histogram.restype = C.c_int
         L.cgs_mi_histogram.argtypes = [P(CgsImage), P(CgsImage), P(C.c_float), C.c_int32, C.c_void_p, C.c_void_p]
+        L.cgs_covariance.restype = C.c_int
+        L.cgs_covariance.argtypes = [P(CgsGrid), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
         L.cgs_status_string.restype = C.c_char_p
         L.cgs_status_string.argtypes = [C.c_int]
         L.cgs_last_error.restype = C.c_char_p

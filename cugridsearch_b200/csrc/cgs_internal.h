@@ -1,9 +1,36 @@
 // cgs_internal.h -- declarations shared by the library's translation units.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <string>
+
 #include "cgs_kernels.cuh"
 
 namespace cgs {
+
+// Host helpers of cgs_search.cu shared with the other C-ABI translation units.
+cgs_status fail(cgs_status s, const std::string &msg);   // sets cgs_last_error()
+cgs_status cuda_fail(cudaError_t e, const char *what);   // CUDA error -> status + message
+cgs_status get_pool(int dev, cudaMemPool_t *out);        // the device's scratch pool
+
+struct DeviceInfo {
+    int dev = -1;
+    int sms = 0;
+    int major = 0;
+    int tex_align = 512;
+    int tex_pitch_align = 32;
+};
+cgs_status device_info(DeviceInfo *d);  // current device; fails unless sm_100
+
+// CudaGrid's increments and element count (float count x int increment, truncated).
+void grid_increments(const cgs_grid &g, int32_t inc[8], int64_t *num);
+cgs_status check_grid(const cgs_grid *g);
+
+#define CGS_CUDA(call, what)                                    \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cgs::cuda_fail(e_, what); \
+    } while (0)
 
 // Kernel of a pixel-loop cost for (channels, points per warp, warps per CTA), or null.
 using KernelGetter = const void *(*)(int C, int G, int NW);

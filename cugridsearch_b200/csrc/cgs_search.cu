@@ -17,22 +17,16 @@ namespace cgs {
 
 static thread_local std::string g_last_error;
 
-static cgs_status fail(cgs_status s, const std::string &msg) {
+cgs_status fail(cgs_status s, const std::string &msg) {
     g_last_error = msg;
     return s;
 }
 
-static cgs_status cuda_fail(cudaError_t e, const char *what) {
+cgs_status cuda_fail(cudaError_t e, const char *what) {
     if (e == cudaErrorMemoryAllocation)
         return fail(CGS_ERROR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
     return fail(CGS_ERROR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define CGS_CUDA(call, what)                       \
-    do {                                           \
-        cudaError_t e_ = (call);                   \
-        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-    } while (0)
 
 // ---------------------------------------------------------------- device memory pool
 
@@ -44,7 +38,7 @@ struct DevicePool {
 };
 static DevicePool g_pools;
 
-static cgs_status get_pool(int dev, cudaMemPool_t *out) {
+cgs_status get_pool(int dev, cudaMemPool_t *out) {
     std::lock_guard<std::mutex> lock(g_pools.mu);
     if (dev < 0 || dev >= 64) return fail(CGS_ERROR_NO_DEVICE, "device ordinal out of range");
     if (!g_pools.pool[dev]) {
@@ -63,15 +57,7 @@ static cgs_status get_pool(int dev, cudaMemPool_t *out) {
     return CGS_SUCCESS;
 }
 
-struct DeviceInfo {
-    int dev = -1;
-    int sms = 0;
-    int major = 0;
-    int tex_align = 512;
-    int tex_pitch_align = 32;
-};
-
-static cgs_status device_info(DeviceInfo *d) {
+cgs_status device_info(DeviceInfo *d) {
     CGS_CUDA(cudaGetDevice(&d->dev), "cudaGetDevice");
     CGS_CUDA(cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, d->dev), "cudaDeviceGetAttribute");
     CGS_CUDA(cudaDeviceGetAttribute(&d->major, cudaDevAttrComputeCapabilityMajor, d->dev), "cudaDeviceGetAttribute");
@@ -86,7 +72,7 @@ static cgs_status device_info(DeviceInfo *d) {
 
 // CudaGrid dimensional increments and element count exactly as the reference computes
 // them: float count times int increment, truncated to int32 (cudaGridSearch.cuh:89-98, 168-172).
-static void grid_increments(const cgs_grid &g, int32_t inc[8], int64_t *num) {
+void grid_increments(const cgs_grid &g, int32_t inc[8], int64_t *num) {
     inc[0] = 1;
     for (int a = 1; a < 8; a++) inc[a] = (a < g.dims) ? (int32_t)(g.count[a - 1] * (float)inc[a - 1]) : 0;
     int32_t total = 1;
@@ -499,7 +485,7 @@ static cgs_status check_image(const cgs_image *im, const char *name) {
     return CGS_SUCCESS;
 }
 
-static cgs_status check_grid(const cgs_grid *g) {
+cgs_status check_grid(const cgs_grid *g) {
     if (!g) return fail(CGS_ERROR_INVALID_VALUE, "grid is null");
     if (g->dims < 1 || g->dims > 8) return fail(CGS_ERROR_INVALID_VALUE, "grid dims must be 1..8");
     for (int a = 0; a < g->dims; a++) {

@@ -160,6 +160,19 @@ cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, c
 cgs_status cgs_search_noalloc(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
                               const cgs_options *options, float *costs, cgs_argmin *result, cgs_stream_t stream);
 
+/* CudaGridSearcher::covariance_by_value -> calculateCovariance_by_value
+ * (src/gpu/cudaGridSearch.cuh:316-419, 768-794): curvature of the cost surface around the
+ * grid minimum.  With f_min the lowest cost below zero (lowest index on ties; 0 at index 0
+ * when no cost is negative) at grid point x_min, every other grid point x with cost f
+ * (0 read as -1e-9) contributes g g^T, g = (x - x_min) s / |x - x_min|,
+ * s = (log|f_min| - log|f|) / |x - x_min|, unless s < 0.
+ *   costs : DEVICE array of the first n costs of the grid (n <= element count), as the
+ *           cost tensor of cgs_search.
+ *   covar : DEVICE array of dims x dims doubles, row-major, overwritten with the sum (the
+ *           reference adds into a caller-initialised float matrix; the caller adds).
+ * The terms are summed in double in a fixed order (deterministic). */
+cgs_status cgs_covariance(const cgs_grid *grid, const float *costs, uint64_t n, double *covar, cgs_stream_t stream);
+
 /* Joint histogram of the MI cost (CGS_COST_MI sampling: centred homography of params, the
  * calcNCC pixel loop) at one parameter vector: hist[bf * bins + bm] counts the (pixel, channel)
  * samples whose fixed value falls in bin bf and moving value in bin bm, bin = floor(v * bins / 256)

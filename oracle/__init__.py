@@ -85,6 +85,7 @@ def lib():
             L.og_params_to_h_norm.argtypes = [P(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_float)]
             L.og_new_coord.argtypes = [P(C.c_float), C.c_int, C.c_int, P(C.c_float), P(C.c_float)]
             L.og_bilinear_probe.argtypes = [P(OgImage), C.c_float, C.c_float, C.c_int, P(C.c_float)]
+            L.og_covariance.argtypes = [P(OgGrid), P(C.c_float), C.c_int64, P(C.c_double), P(C.c_float)]
             L.og_search.restype = C.c_int
             L.og_search.argtypes = [C.c_int, P(OgGrid), C.c_int, P(OgImage), P(OgImage), P(OgOpts),
                                     C.c_int64, C.c_int64, C.c_int64, P(C.c_float), P(C.c_double), C.c_int]
@@ -215,6 +216,16 @@ def search(name: str, g: OgGrid, mov: Image, fix: Image, o: OgOpts | None = None
     if rc != 0:
         raise ValueError("og_search rejected its arguments")
     return c32, c64
+
+
+def covariance(g: OgGrid, costs: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """(double-accumulated, reference float-accumulated) covariance of a cost array."""
+    c = np.ascontiguousarray(costs, dtype=np.float32)
+    d = g.dims
+    o64 = np.zeros(d * d, dtype=np.float64)
+    o32 = np.zeros(d * d, dtype=np.float32)
+    lib().og_covariance(C.byref(g), _fptr(c), c.size, o64.ctypes.data_as(C.POINTER(C.c_double)), _fptr(o32))
+    return o64.reshape(d, d), o32.reshape(d, d)
 
 
 def ref_cost(name: str, params, mov: Image, fix: Image) -> float:

@@ -368,3 +368,45 @@ int og_search(int cost, const og_grid *g, int use_fma, const og_image *mov, cons
     (void)threads;
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Covariance around the grid minimum (src/gpu/cudaGridSearch.cuh:316-419)     */
+/* ------------------------------------------------------------------------- */
+
+void og_covariance(const og_grid *g, const float *costs, int64_t n, double *out_f64, float *out_ref) {
+    const int D = g->dims;
+    for (int i = 0; i < D * D; i++) {
+        if (out_f64) out_f64[i] = 0.0;
+        if (out_ref) out_ref[i] = 0.0f;
+    }
+    float fmin = 0.0f;
+    int64_t imin = 0;
+    for (int64_t t = 0; t < n; t++) /* func_precision min_val = 0; strict '<' */
+        if (costs[t] < fmin) {
+            fmin = costs[t];
+            imin = t;
+        }
+    float xm[8], x[8];
+    og_grid_point(g, imin, 1, xm);
+    const float lmin = logf(fabsf(fmin));
+    for (int64_t t = 0; t < n; t++) {
+        if (t == imin) continue;
+        og_grid_point(g, t, 1, x);
+        float f = costs[t];
+        if (f == 0.0f) f = -1e-9f;
+        float d[8], gv[8], len = 0.0f;
+        for (int a = 0; a < D; a++) {
+            d[a] = x[a] - xm[a];
+            len = fmaf(d[a], d[a], len); /* length += d * d, fused by the device build */
+        }
+        len = sqrtf(len);
+        const float slope = (lmin - logf(fabsf(f))) * (1.0f / len);
+        if (slope < 0.0f) continue;
+        for (int a = 0; a < D; a++) gv[a] = (d[a] * slope) / len;
+        for (int r = 0; r < D; r++)
+            for (int c = 0; c < D; c++) {
+                if (out_f64) out_f64[r * D + c] += (double)gv[r] * (double)gv[c];
+                if (out_ref) out_ref[r * D + c] = fmaf(gv[r], gv[c], out_ref[r * D + c]);
+            }
+    }
+}

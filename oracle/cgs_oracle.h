@@ -92,6 +92,14 @@ int og_search(int cost, const og_grid *g, int use_fma, const og_image *mov, cons
               const og_opts *opts, int64_t first, int64_t count, int64_t stride,
               float *costs32, double *costs64, int threads);
 
+/* calculateCovariance_by_value (src/gpu/cudaGridSearch.cuh:316-419) over the first n costs
+ * of grid g: f_min = lowest cost below zero (strict '<' from 0 at index 0), then for every
+ * other index the term g g^T with the reference's per-term float operations as its device
+ * build evaluates them (fused |x - x_min|^2).  out_f64 (nullable): terms summed in double;
+ * out_ref (nullable): summed sequentially in float with fused multiply-adds, the
+ * reference's own accumulation.  Both dims x dims row-major, overwritten. */
+void og_covariance(const og_grid *g, const float *costs, int64_t n, double *out_f64, float *out_ref);
+
 #ifdef __cplusplus
 }
 #endif
