@@ -124,6 +124,9 @@ def ref():
                                         C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                         C.c_int, C.c_int64, C.c_int64, C.c_int64, P(C.c_float), C.c_int]
             L.cgsref_max_threads.restype = C.c_int
+            L.cgsref_device_grid_points.restype = C.c_int
+            L.cgsref_device_grid_points.argtypes = [C.c_int, P(C.c_float), P(C.c_float), P(C.c_float),
+                                                    P(C.c_int64), C.c_int, P(C.c_float), P(C.c_float)]
             _ref = L
     return _ref
 
@@ -234,6 +237,21 @@ def ref_cost(name: str, params, mov: Image, fix: Image) -> float:
     mh, mw, _ = mov.arr.shape
     return ref().cgsref_eval(COSTS[name], _fptr(p), PIX[mov.arr.dtype], mov.padded.ctypes.data, mh, mw,
                              fix.padded.ctypes.data, h, w, c)
+
+
+def ref_device_grid_points(start, end, count, indices):
+    """Grid points decoded by the reference's own CudaGrid on the GPU (dims 2 or 8, counts >= 2):
+    (points[n, dims], matrix[4, dims] = start, end, resolution, count after the updates)."""
+    d = len(start)
+    st, en, ct = (np.ascontiguousarray(v, dtype=np.float32) for v in (start, end, count))
+    idx = np.ascontiguousarray(indices, dtype=np.int64)
+    out = np.zeros((len(idx), d), dtype=np.float32)
+    mat = np.zeros((4, d), dtype=np.float32)
+    rc = ref().cgsref_device_grid_points(d, _fptr(st), _fptr(en), _fptr(ct),
+                                         idx.ctypes.data_as(C.POINTER(C.c_int64)), len(idx), _fptr(out), _fptr(mat))
+    if rc != 0:
+        raise RuntimeError(f"cgsref_device_grid_points failed ({rc})")
+    return out, mat
 
 
 def ref_search(name: str, g: OgGrid, mov: Image, fix: Image, first: int = 0, count: int | None = None,

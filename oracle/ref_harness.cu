@@ -75,6 +75,40 @@ float eval_p(int cost, const float *params, const void *mov, int mh, int mw, con
 
 }  // namespace
 
+/* The reference's own grid on the DEVICE: CudaGrid<float, D> with caller-allocated data,
+ * setStartPoint / setEndPoint / setNumSamples (each runs updateProcess<<<1,1>>>), then
+ * getGridPoint (gridPointProcess<<<1,1>>>) for each index.  Compiled by nvcc with its
+ * default flags, as the reference's drivers are, so the device rounding of the decode
+ * (start + i * res, contracted or not) is the reference's.  No axis may end up with one
+ * sample (count < 2, or |end - start| < 1e-7 count, which updateProcess collapses): for
+ * such an axis updateProcess reads start_point()[-1] (cudaGridSearch.cuh:266), before
+ * the allocation.  matrix (4 x D floats) receives the grid after the updates.  Returns 0 on
+ * success, 1 on a CUDA error, 2 on a bad argument. */
+template <unsigned int D>
+static int device_grid_points(const float *start, const float *end, const float *count, const int64_t *idx, int n,
+                              float *out, float *matrix) {
+    for (unsigned int a = 0; a < D; a++)  // no axis may collapse to one sample
+        if (!(count[a] >= 2.0f) || !((double)std::fabs(end[a] - start[a]) >= 1.0e-7 * (double)count[a])) return 2;
+    CudaGrid<float, D> g;
+    if (cudaMalloc(&g.data(), g.bytesSize()) != cudaSuccess) return 1;
+    // zeroed first: each setter runs updateProcess over all rows, and with uninitialised
+    // counts or ends an axis could look collapsed before its own setter has run
+    if (cudaMemset(g.data(), 0, g.bytesSize()) != cudaSuccess) return 1;
+    g.setStartPoint(std::vector<float>(start, start + D));
+    g.setEndPoint(std::vector<float>(end, end + D));
+    g.setNumSamples(std::vector<float>(count, count + D));
+    int rc = 0;
+    if (cudaMemcpy(matrix, g.data(), g.bytesSize(), cudaMemcpyDeviceToHost) != cudaSuccess) rc = 1;
+    for (int k = 0; k < n && rc == 0; k++) {
+        float pt[D];
+        g.getGridPoint(pt, (int)idx[k]);
+        for (unsigned int a = 0; a < D; a++) out[(size_t)k * D + a] = pt[a];
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = 1;
+    cudaFree(g.data());
+    return rc;
+}
+
 extern "C" {
 
 /* One reference functor evaluation. pix: 0 = float, 1 = uint8_t, 2 = double, 3 = uint16_t. */
@@ -149,5 +183,14 @@ int cgsref_search(int cost, int dims, const float *start, const float *res, cons
 }
 
 int cgsref_max_threads(void) { return omp_get_max_threads(); }
+
+int cgsref_device_grid_points(int dims, const float *start, const float *end, const float *count, const int64_t *idx,
+                              int n, float *out, float *matrix) {
+    switch (dims) {
+        case 2: return device_grid_points<2>(start, end, count, idx, n, out, matrix);
+        case 8: return device_grid_points<8>(start, end, count, idx, n, out, matrix);
+        default: return 2;
+    }
+}
 
 }  // extern "C"
