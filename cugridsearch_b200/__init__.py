@@ -24,13 +24,13 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from ._abi import COSTS, CgsArgmin, CgsError, CgsGrid, CgsImage, CgsOptions, check
+from ._abi import COSTS, CgsArgmin, CgsBatchPlan, CgsError, CgsGrid, CgsImage, CgsOptions, CgsPair, CgsTuneEntry, check
 
 __all__ = [
     "CudaGrid", "CudaImage", "CudaTensor", "CudaGridSearcher", "Argmin", "search", "argmin",
     "COSTS", "CgsError", "library", "averageAbsoluteDifference", "averageAbsoluteDifferenceH",
     "sumOfAbsoluteDifferences", "sumOfAbsoluteDifferences_by_reference", "calcSQD", "calcNCC",
-    "calcSQDAlt", "calcNCCAlt", "calcMIAlt", "ZNCC", "MI",
+    "calcSQDAlt", "calcNCCAlt", "calcMIAlt", "ZNCC", "MI", "Batch", "BatchPair", "BatchPlan",
 ]
 
 # Cost selectors named after the reference functors (the device function pointer the
@@ -316,3 +316,101 @@ class CudaGridSearcher:
             covar_matrix += cov.astype(covar_matrix.dtype).reshape(covar_matrix.shape)
             return covar_matrix
         return cov
+
+
+@dataclass
+class BatchPlan:
+    """Launch plan of the batch kernel (cgs_batch_plan): grid points per warp (1, 2, 4, 8),
+    warps per block (4, 8, 16) and whether a block's warps share points (block_split: MI
+    histograms per block) or own them (MI histograms per warp)."""
+    points_per_warp: int = 2
+    warps_per_block: int = 16
+    block_split: int = 0
+
+    def to_c(self) -> CgsBatchPlan:
+        return CgsBatchPlan(self.points_per_warp, self.warps_per_block, self.block_split, 0)
+
+    @staticmethod
+    def from_c(p: CgsBatchPlan) -> "BatchPlan":
+        return BatchPlan(int(p.points_per_warp), int(p.warps_per_block), int(p.block_split))
+
+
+@dataclass
+class BatchPair:
+    """One pair of a batch: images, grid, cost options, an optional cost dump and a device
+    result buffer (see :func:`result_buffer`)."""
+    cost: str
+    moving: CudaImage
+    fixed: CudaImage
+    grid: CudaGrid
+    result: object
+    costs: object = None
+    mi_bins: int = 0
+    overlap_gate: float = 0.0
+    exact_samples: bool | None = None
+
+    def to_c(self) -> CgsPair:
+        opt = _options(self.cost, self.mi_bins, self.overlap_gate, exact_samples=self.exact_samples)
+        return CgsPair(self.moving.img, self.fixed.img, self.grid.g, opt,
+                       self.costs.data_ptr() if self.costs is not None else None, self.result.data_ptr())
+
+
+class Batch:
+    """Many pairs in one persistent launch (cgs_batch_*): the pairs' images, dumps and
+    results are bound at creation; :meth:`launch` replays the recorded CUDA graph."""
+
+    def __init__(self, pairs: list[BatchPair], plan: BatchPlan | None = None):
+        self.pairs = list(pairs)  # keeps the tensors alive
+        arr = (CgsPair * len(self.pairs))(*[p.to_c() for p in self.pairs])
+        h = C.c_void_p(None)
+        cp = C.byref(plan.to_c()) if plan is not None else None
+        check(_abi.load().cgs_batch_create(arr, len(self.pairs), cp, C.byref(h)))
+        self._h = h
+
+    def launch(self, stream=None) -> None:
+        check(_abi.load().cgs_batch_launch(self._h, _stream_handle(stream)))
+
+    @property
+    def plan(self) -> BatchPlan:
+        p = CgsBatchPlan()
+        check(_abi.load().cgs_batch_get_plan(self._h, C.byref(p)))
+        return BatchPlan.from_c(p)
+
+    @plan.setter
+    def plan(self, plan: BatchPlan) -> None:
+        check(_abi.load().cgs_batch_set_plan(self._h, C.byref(plan.to_c())))
+
+    def autotune(self, sample_points: int = 4096) -> tuple[BatchPlan, list[tuple[BatchPlan, float, int]]]:
+        """Times all 24 plans on the first ``sample_points`` points of every pair, applies the
+        fastest and returns it with every (plan, ms, status) measurement."""
+        entries = (CgsTuneEntry * 32)()
+        n = C.c_int32(0)
+        best = CgsBatchPlan()
+        check(_abi.load().cgs_batch_autotune(self._h, int(sample_points), entries, 32, C.byref(n), C.byref(best)))
+        table = [(BatchPlan.from_c(e.plan), float(e.ms), int(e.status)) for e in entries[: n.value]]
+        return BatchPlan.from_c(best), table
+
+    def pair_times(self) -> tuple[np.ndarray, np.ndarray]:
+        """(start, end) device time stamps in ns of each pair's first and last task in the
+        last launch (waits for it)."""
+        n = len(self.pairs)
+        a, b = (C.c_uint64 * n)(), (C.c_uint64 * n)()
+        check(_abi.load().cgs_batch_pair_times(self._h, a, b))
+        return np.array(list(a), dtype=np.uint64), np.array(list(b), dtype=np.uint64)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _abi.load().cgs_batch_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

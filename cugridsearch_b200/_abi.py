@@ -32,6 +32,8 @@ EXPORTS = [
     "cgs_grid_update", "cgs_grid_num_elements", "cgs_grid_point", "cgs_search",
     "cgs_argmin_f32", "cgs_search_sync", "cgs_status_string", "cgs_last_error", "cgs_version",
     "cgs_mi_histogram", "cgs_search_noalloc", "cgs_covariance",
+    "cgs_batch_create", "cgs_batch_launch", "cgs_batch_set_plan", "cgs_batch_get_plan", "cgs_batch_autotune",
+    "cgs_batch_pair_times", "cgs_batch_destroy", "cgs_search_batched", "cgs_autotune",
 ]
 
 
@@ -53,6 +55,20 @@ class CgsOptions(C.Structure):
 class CgsArgmin(C.Structure):
     _fields_ = [("cost", C.c_float), ("valid", C.c_int32), ("index", C.c_int64),
                 ("params", C.c_float * 8), ("status", C.c_int32), ("reserved", C.c_int32)]
+
+
+class CgsPair(C.Structure):
+    _fields_ = [("moving", CgsImage), ("fixed", CgsImage), ("grid", CgsGrid), ("options", CgsOptions),
+                ("costs", C.c_void_p), ("result", C.c_void_p)]
+
+
+class CgsBatchPlan(C.Structure):
+    _fields_ = [("points_per_warp", C.c_int32), ("warps_per_block", C.c_int32), ("block_split", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class CgsTuneEntry(C.Structure):
+    _fields_ = [("plan", CgsBatchPlan), ("ms", C.c_float), ("status", C.c_int32)]
 
 
 class CgsError(RuntimeError):
@@ -96,6 +112,25 @@ def load() -> C.CDLL:
         L.cgs_mi_histogram.argtypes = [P(CgsImage), P(CgsImage), P(C.c_float), C.c_int32, C.c_void_p, C.c_void_p]
         L.cgs_covariance.restype = C.c_int
         L.cgs_covariance.argtypes = [P(CgsGrid), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.cgs_batch_create.restype = C.c_int
+        L.cgs_batch_create.argtypes = [P(CgsPair), C.c_int32, P(CgsBatchPlan), P(C.c_void_p)]
+        L.cgs_batch_launch.restype = C.c_int
+        L.cgs_batch_launch.argtypes = [C.c_void_p, C.c_void_p]
+        L.cgs_batch_set_plan.restype = C.c_int
+        L.cgs_batch_set_plan.argtypes = [C.c_void_p, P(CgsBatchPlan)]
+        L.cgs_batch_get_plan.restype = C.c_int
+        L.cgs_batch_get_plan.argtypes = [C.c_void_p, P(CgsBatchPlan)]
+        L.cgs_batch_autotune.restype = C.c_int
+        L.cgs_batch_autotune.argtypes = [C.c_void_p, C.c_int32, P(CgsTuneEntry), C.c_int32, P(C.c_int32),
+                                         P(CgsBatchPlan)]
+        L.cgs_batch_pair_times.restype = C.c_int
+        L.cgs_batch_pair_times.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
+        L.cgs_batch_destroy.restype = C.c_int
+        L.cgs_batch_destroy.argtypes = [C.c_void_p]
+        L.cgs_search_batched.restype = C.c_int
+        L.cgs_search_batched.argtypes = [P(CgsPair), C.c_int32, P(CgsBatchPlan), C.c_void_p]
+        L.cgs_autotune.restype = C.c_int
+        L.cgs_autotune.argtypes = [P(CgsPair), C.c_int32, C.c_int32, P(CgsBatchPlan)]
         L.cgs_status_string.restype = C.c_char_p
         L.cgs_status_string.argtypes = [C.c_int]
         L.cgs_last_error.restype = C.c_char_p

@@ -12,6 +12,7 @@ import argparse
 import concurrent.futures as cf
 import hashlib
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -39,14 +40,33 @@ def _sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-def _headers():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))) + \
-        [os.path.join(INCLUDE, "cugridsearch_b200.h")]
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s*"([^"]+)"', re.M)
+
+
+def _deps(src: str) -> list[str]:
+    """The file and every project header it includes, transitively (quoted includes
+    resolved against the including file's folder, csrc/ and include/)."""
+    seen: list[str] = []
+    todo = [os.path.abspath(src)]
+    while todo:
+        f = todo.pop()
+        if f in seen:
+            continue
+        seen.append(f)
+        with open(f) as fh:
+            text = fh.read()
+        for name in _INCLUDE_RE.findall(text):
+            for base in (os.path.dirname(f), CSRC, INCLUDE):
+                cand = os.path.abspath(os.path.join(base, name))
+                if os.path.exists(cand):
+                    todo.append(cand)
+                    break
+    return sorted(seen)
 
 
 def _stamp(src: str, extra: list[str]) -> str:
     h = hashlib.sha256()
-    for f in [src] + _headers():
+    for f in _deps(src):
         with open(f, "rb") as fh:
             h.update(fh.read())
     h.update(" ".join(NVFLAGS + ARCH + extra).encode())

@@ -26,6 +26,48 @@ cgs_status device_info(DeviceInfo *d);  // current device; fails unless sm_100
 void grid_increments(const cgs_grid &g, int32_t inc[8], int64_t *num);
 cgs_status check_grid(const cgs_grid *g);
 
+// Staging-kernel parameters of one pair (prep_kernel / batch_prep_kernel).
+struct PrepParams {
+    const void *mov_src;
+    const void *fix_src;
+    int32_t mov_pix, fix_pix;
+    int32_t mh, mw, fh, fw, c;
+    float *mov_dst;
+    float *fix_dst;
+    int64_t mplane, fplane;
+    int32_t mpitch, fpitch;
+    unsigned long long *key;
+    unsigned int *done;
+    unsigned int *status;
+    float *vmax;  // zeroed before the launch
+    int32_t fix_alias;   // stage the fixed image like the moving one (scanline functors)
+    float *row_table;    // calcMIAlt row values, or null
+    int32_t rowsf;
+};
+
+// Staged layout of a moving/fixed image pair inside one scratch block.
+struct Staging {
+    int32_t mpitch = 0, fpitch = 0;
+    int64_t mplane = 0, fplane = 0;
+    size_t mov_off = 0, fix_off = 0, rows_off = 0, bytes = 0;
+};
+
+Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align,
+                       bool fix_alias = false, bool row_table = false);
+char *staging_origin(void *scratch, int tex_align);  // first tex_align boundary of a block
+bool exact_samples(int cost, int flags);             // sampling mode of a request
+
+// Request validation and kernel parameters shared by every pixel-loop entry point.
+cgs_status check_request(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options *options,
+                         int *mi_bins);
+cgs_status fill_params(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options &o,
+                       int mi_bins, SearchParams *p, int64_t *n64);
+int64_t set_chunks(SearchParams *p, const Staging &st, int C, int fix_h);
+PrepParams make_prep(const cgs_image *mov, const cgs_image *fix, const Staging &st, char *sb, float *mstage,
+                     float *fstage);
+size_t acc_bytes(int cost, int G, int NW, bool block_split, int mi_bins);
+const void *batch_prep_kernel_fn();  // batch_prep_kernel(const PrepParams *), grid (x, pairs)
+
 #define CGS_CUDA(call, what)                                    \
     do {                                                        \
         cudaError_t e_ = (call);                                \

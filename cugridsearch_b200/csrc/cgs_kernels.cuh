@@ -43,8 +43,9 @@ struct SearchParams {
     int32_t perm[8];     // evaluation order, perm[0] varies fastest
     int32_t dims;
     int32_t natural;     // 1: ordinal == grid index (non-integer counts or forced)
+    int32_t cost;        // cgs_cost (read by the batch kernel to pick the task body)
     uint32_t n;          // number of grid points
-    uint32_t num_tasks;
+    uint32_t num_tasks;  // tasks of this search; the one that completes the count writes the result
     // images
     Plane mov, fix;
     float mov_wf, mov_hf;
@@ -200,7 +201,7 @@ struct FixTerms {
 };
 
 template <int COST>
-__device__ __forceinline__ FixTerms fix_terms(float f, const SearchParams &p) {
+__device__ __forceinline__ FixTerms fix_terms(float f, float sB, int bins) {
     FixTerms t;
     t.f = f;
     t.a = 0.0f;
@@ -213,8 +214,7 @@ __device__ __forceinline__ FixTerms fix_terms(float f, const SearchParams &p) {
         t.a = f - kZnccShift;
         t.b = t.a * t.a;
     } else if constexpr (COST == CGS_COST_MI) {
-        const float sB = (float)p.mi_bins * (1.0f / 256.0f);
-        t.bin = min(max((int)floorf(f * sB), 0), p.mi_bins - 1);
+        t.bin = min(max((int)floorf(f * sB), 0), bins - 1);  // sB = bins / 256
     }
     return t;
 }
@@ -344,7 +344,7 @@ static __device__ void write_result(const SearchParams &p) {
     *p.result = r;
 }
 
-// ---------------------------------------------------------------- the kernel
+// ---------------------------------------------------------------- one task of a persistent CTA
 
 // MI bin guard of one grid point: coordinate bounds scaled to bin units (sgx, sgy) and the
 // widest fractional tap weight that keeps the sample in its cell (hx, hy).
@@ -359,227 +359,269 @@ struct ExactSlot {
     float B, C2, D2, pad;
 };
 
-// NW warps per CTA; 512 / (32 NW) CTAs share an SM (two CTAs of 8 warps hide each
-// other's chunk barriers).
-template <int COST, int C, int G, int NW, bool TEX = (COST != CGS_COST_MI)>
-__global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_constant__ SearchParams p) {
-    extern __shared__ __align__(128) unsigned char smem[];
+// Shared memory of a persistent search CTA: kStages mbarriers, the per-warp argmin keys, the
+// abort flag, kStages fixed-image stages, the grid points' exact-path slots [NW][G], the
+// per-(warp, point) term counts [NW][G], then the running sums [NW][G][NA][32] or the MI
+// histograms ([NW][G] of them when each warp owns its points, [G] when the warps share them).
+struct CtaSmem {
+    uint64_t *bars;
+    unsigned long long *wbest;
+    int *abort_flag;
+    float *stages;
+    int stage_floats;
+    ExactSlot *slots;
+    int *cnts;
+    float *acc;
+};
+
+__host__ __device__ constexpr size_t cta_smem_head(int NW) { return 128 + 8 * (size_t)NW; }
+
+// Bytes of dynamic shared memory of a CTA; acc_bytes is the sums or histograms region.
+__host__ __device__ constexpr size_t cta_smem_bytes(int G, int NW, size_t stage_bytes, size_t acc_bytes) {
+    return cta_smem_head(NW) + kStages * stage_bytes + (size_t)NW * G * (sizeof(ExactSlot) + sizeof(int)) + acc_bytes;
+}
+
+template <int G, int NW>
+__device__ __forceinline__ CtaSmem carve_smem(unsigned char *smem, int stage_floats) {
+    CtaSmem s;
+    s.bars = reinterpret_cast<uint64_t *>(smem);
+    s.wbest = reinterpret_cast<unsigned long long *>(smem + 64);
+    s.abort_flag = reinterpret_cast<int *>(smem + 64 + 8 * NW);
+    s.stages = reinterpret_cast<float *>(smem + cta_smem_head(NW));
+    s.stage_floats = stage_floats;
+    s.slots = reinterpret_cast<ExactSlot *>(s.stages + kStages * stage_floats);
+    s.cnts = reinterpret_cast<int *>(s.slots + NW * G);
+    s.acc = reinterpret_cast<float *>(s.cnts + NW * G);
+    return s;
+}
+
+// Bulk copy of chunk `chunk` of a pair's staged fixed image (rows chunk * R ..) into stage
+// it % kStages; plane c of the chunk lands at c * R * pitch.  Thread 0 only.
+template <int C>
+__device__ __forceinline__ void issue_chunk(const SearchParams &p, const CtaSmem &sm, uint32_t it, int chunk) {
+    const int R = p.chunk_rows, fpitch = p.fix.pitch;
+    const int r0 = chunk * R;
+    const int rows = min(R, p.fix.h - r0);
+    const uint32_t bytes = (uint32_t)rows * (uint32_t)fpitch * 4u;
+    float *dst = sm.stages + (it % kStages) * sm.stage_floats;
+    uint64_t *bar = &sm.bars[it % kStages];
+    fence_proxy_async_smem();  // the stage's previous reads (generic proxy) before the async refill
+    mbar_arrive_expect_tx(bar, bytes * C);
+#pragma unroll
+    for (int c = 0; c < C; c++)
+        bulk_g2s(dst + c * R * fpitch, p.fix.data + c * p.fix.plane + (int64_t)r0 * fpitch, bytes, bar);
+}
+
+// Completion of a task (thread 0, after the CTA barrier that follows the task's argmin):
+// fold the CTA's key into the pair's, count the task, and let the pair's last task write the
+// decoded result.  `tasks` > 1 retires tasks that an aborted CTA will not run.
+__device__ __forceinline__ void retire_tasks(const SearchParams &p, unsigned long long key, uint32_t tasks,
+                                             bool timed_out) {
+    if (key != ~0ull) atomicMin(p.key, key);
+    if (timed_out) atomicOr(p.status, (unsigned)CGS_ERROR_DEVICE_TIMEOUT);
+    __threadfence();
+    const unsigned int old = atomicAdd(p.done, tasks);
+    if (old + tasks == p.num_tasks) {
+        __threadfence();
+        write_result(p);
+    }
+}
+
+// One task: the G (BSPLIT) or NW * G grid points of ordinals task * points-per-task .., over
+// every chunk of the fixed image.
+//   BSPLIT = false: warp w owns G consecutive points and sweeps every pixel for them (lane l
+//                   takes every 32nd pixel); MI histograms are private to a (warp, point).
+//   BSPLIT = true:  the NW warps share G points and split the pixels (lane l of warp w takes
+//                   pixels w * 32 + l + k * 32 NW); MI histograms are per (block, point).
+// Per-lane partial sums are folded per chunk into shared memory (two-level summation).  With
+// BSPLIT = false the summation order of a point does not depend on G or NW, so costs are
+// bit-identical across those tunings.  Thread 0 calls prod.after_chunk(it) after each chunk's
+// barrier to refill the released stage.  Returns false if a bounded wait gave up (the CTA
+// stops; the task is not retired).
+template <int COST, int C, int G, int NW, bool TEX, bool BSPLIT, class Prod>
+__device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, const CtaSmem &sm, uint32_t &it,
+                                         Prod &prod) {
     constexpr int NA = AccN<COST>::value;
     constexpr bool kMI = (COST == CGS_COST_MI);
     constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
     // taps: one texture gather per sample (fewer instructions); MI, whose extra bin-guard work
     // leaves less latency tolerance, measured faster with four cached global loads
     constexpr bool kTexTaps = TEX;
-
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    unsigned long long *wbest = reinterpret_cast<unsigned long long *>(smem + 64);
-    int *abort_flag = reinterpret_cast<int *>(smem + 64 + 8 * NW);
-    float *stages = reinterpret_cast<float *>(smem + 128 + 8 * NW);
-    const int fpitch = p.fix.pitch;
-    const int R = p.chunk_rows;
-    const int stage_floats = R * fpitch * C;
-    ExactSlot *slots = reinterpret_cast<ExactSlot *>(stages + kStages * stage_floats);
-    // per-task running sums, [warp][g][j][lane]: updated once per chunk (two-level summation)
-    float *totals = reinterpret_cast<float *>(slots + NW * G);
-    uint32_t *hist_base = reinterpret_cast<uint32_t *>(totals + (kMI ? 0 : NW * G * NA * 32));
-    const int B = p.mi_bins;
-    const int hstride = B + 1;                 // row stride (bank-conflict padding)
-    const int hsize = (B + 1) * (B + 1);       // + a row/column for the marginals
+    constexpr int PSTEP = BSPLIT ? NW * 32 : 32;  // pixel stride of a lane
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int fw = p.fix.w, fh = p.fix.h;
+    const int fpitch = p.fix.pitch;
+    const int R = p.chunk_rows;
+    const int num_chunks = p.num_chunks;
     const int mpitch = p.mov.pitch;
     const int64_t mplane = p.mov.plane;
     const float mrows = (float)(p.mov.h + 1);  // texture rows per plane
     const float *__restrict__ mdata = p.mov.data;
-    const float hw = 0.5f * p.mov_wf, hh = 0.5f * p.mov_hf;
+    const cudaTextureObject_t mtex = p.mov_tex;
+    const float mov_wf = p.mov_wf, mov_hf = p.mov_hf;
+    const float hw = 0.5f * mov_wf, hh = 0.5f * mov_hf;
+    const int B = p.mi_bins;
+    const int hstride = B + 1;            // row stride (bank-conflict padding)
+    const int hsize = (B + 1) * (B + 1);  // + a row/column for the marginals
     const float sB = (float)B * (1.0f / 256.0f);
     // value-rounding allowance of the MI bin guard: fast and exact bilinear values of the
     // same coordinates differ by at most 8u * max|v| (bin units, twice for safety)
     const float gv0 = kMI ? sB * 2.0f * 8.0f * 5.9604645e-8f * (*p.vmax) + 1e-6f : 0.0f;
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) mbar_init(&bars[s], 1);
-        fence_mbar_init();
-        *abort_flag = 0;
-    }
-    __syncthreads();
+    const uint32_t ord0 = BSPLIT ? task * G : (task * NW + warp) * G;
 
-    const uint32_t my_tasks =
-        (p.num_tasks > blockIdx.x) ? (p.num_tasks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
-    const uint32_t total_it = my_tasks * (uint32_t)p.num_chunks;
-
-    auto issue = [&](uint32_t it) {
-        const int chunk = (int)(it % (uint32_t)p.num_chunks);
-        const int r0 = chunk * R;
-        const int rows = min(R, fh - r0);
-        const uint32_t bytes = (uint32_t)rows * (uint32_t)fpitch * 4u;
-        float *dst = stages + (it % kStages) * stage_floats;
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&bars[it % kStages], bytes * C);
+    FastMap fm[G];
+    MiGuard mg[G];  // used by the MI instantiations only
+    uint32_t gidx[G];
+    bool gvalid[G];
+    ExactSlot *my_slots = sm.slots + warp * G;  // BSPLIT: every warp keeps its own copy
 #pragma unroll
-        for (int c = 0; c < C; c++)
-            bulk_g2s(dst + c * R * fpitch, p.fix.data + c * p.fix.plane + (int64_t)r0 * fpitch, bytes,
-                     &bars[it % kStages]);
-    };
-
-    if (threadIdx.x == 0) {
-        for (uint32_t it = 0; it < (uint32_t)kStages && it < total_it; it++) issue(it);
+    for (int g = 0; g < G; g++) {
+        const uint32_t o = ord0 + g;
+        gvalid[g] = o < p.n;
+        int32_t ax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        gidx[g] = gvalid[g] ? ordinal_to_index(p, o, ax) : 0u;
+        float q[8];
+        grid_values(p, ax, q);
+        const float2 cs = p.trig[min(ax[0], kMaxTrig - 1)];
+        const MapCoef kc = make_coef<COST>(q, cs, p);
+        float gx, gy;
+        RowTerms rt;
+        map_guard(kc, p, fm[g], rt, gx, gy);
+        mg[g].sgx = sB * gx;
+        mg[g].sgy = sB * gy;
+        mg[g].hx = 0.5f - gx;
+        mg[g].hy = 0.5f - gy;
+        if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy, rt, kc.B, kc.C2, kc.D2, 0.0f};
     }
 
-    unsigned long long best = ~0ull;
-    uint32_t it = 0;
-    bool aborted = false;
-
-    for (uint32_t k = 0; k < my_tasks && !aborted; k++) {
-        const uint32_t task = blockIdx.x + k * gridDim.x;
-        const uint32_t ord0 = (task * NW + warp) * G;
-
-        FastMap fm[G];
-        MiGuard mg[G];  // used by the MI instantiations only
-        uint32_t gidx[G];
-        bool gvalid[G];
-        ExactSlot *my_slots = slots + warp * G;
+    float *tot = sm.acc + warp * G * NA * 32 + lane;
+    int cnt[G];
 #pragma unroll
-        for (int g = 0; g < G; g++) {
-            const uint32_t o = ord0 + g;
-            gvalid[g] = o < p.n;
-            int32_t ax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            gidx[g] = gvalid[g] ? ordinal_to_index(p, o, ax) : 0u;
-            float q[8];
-            grid_values(p, ax, q);
-            const float2 cs = p.trig[min(ax[0], kMaxTrig - 1)];
-            const MapCoef kc = make_coef<COST>(q, cs, p);
-            float gx, gy;
-            RowTerms rt;
-            map_guard(kc, p, fm[g], rt, gx, gy);
-            mg[g].sgx = sB * gx;
-            mg[g].sgy = sB * gy;
-            mg[g].hx = 0.5f - gx;
-            mg[g].hy = 0.5f - gy;
-            if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy, rt, kc.B, kc.C2, kc.D2, 0.0f};
+    for (int g = 0; g < G; g++) {
+        cnt[g] = 0;
+        if constexpr (!kMI) {
+#pragma unroll
+            for (int j = 0; j < NA; j++) tot[(g * NA + j) * 32] = 0.0f;
         }
-
-        float *tot = totals + warp * G * NA * 32 + lane;
-        int cnt[G];
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-            cnt[g] = 0;
-            if constexpr (!kMI) {
-#pragma unroll
-                for (int j = 0; j < NA; j++) tot[(g * NA + j) * 32] = 0.0f;
-            }
-        }
-        uint32_t *hist = hist_base + (size_t)warp * G * hsize;
-        if constexpr (kMI) {
+    }
+    uint32_t *hist = reinterpret_cast<uint32_t *>(sm.acc) + (BSPLIT ? 0 : (size_t)warp * G * hsize);
+    if constexpr (kMI) {
+        if constexpr (BSPLIT) {
+            for (int i = threadIdx.x; i < G * hsize; i += NW * 32) hist[i] = 0u;
+        } else {
             for (int i = lane; i < G * hsize; i += 32) hist[i] = 0u;
         }
-        __syncwarp();
+    }
+    if constexpr (BSPLIT && kMI) __syncthreads();
+    else __syncwarp();
 
-        for (int ch = 0; ch < p.num_chunks; ch++, it++) {
-            const int stage = (int)(it % kStages);
-            const uint32_t parity = (it / kStages) & 1u;
-            if (!mbar_wait_bounded(&bars[stage], parity, kWaitLimitNs)) *abort_flag = 1;
-            const float *sfix = stages + stage * stage_floats;
-            const int r0 = ch * R;
-            const int rows = min(R, fh - r0);
+    const int pstart = BSPLIT ? warp * 32 + lane : lane;
+    for (int ch = 0; ch < num_chunks; ch++, it++) {
+        const int stage = (int)(it % kStages);
+        const uint32_t parity = (it / kStages) & 1u;
+        if (!mbar_wait_bounded(&sm.bars[stage], parity, kWaitLimitNs)) *sm.abort_flag = 1;
+        const float *sfix = sm.stages + stage * sm.stage_floats;
+        const int r0 = ch * R;
+        const int rows = min(R, fh - r0);
 
-            float part[G][NA];
+        float part[G][NA];
 #pragma unroll
-            for (int g = 0; g < G; g++)
+        for (int g = 0; g < G; g++)
 #pragma unroll
-                for (int j = 0; j < NA; j++) part[g][j] = 0.0f;
+            for (int j = 0; j < NA; j++) part[g][j] = 0.0f;
 
-            if (p.exact_only) {
-                // Exact sampling: coordinates, tap weights and values in the reference's
-                // operation order (calcNewCoordH + valueAt_bilinear), so every sample is the
-                // reference's bit for bit.  Row products B*y, C2*y, D2*y are formed once per row.
-                float ek[G][9];  // A, C1, D1, P, Q, R, S, T, U
+        if (p.exact_only) {
+            // Exact sampling: coordinates, tap weights and values in the reference's
+            // operation order (calcNewCoordH + valueAt_bilinear), so every sample is the
+            // reference's bit for bit.  Row products B*y, C2*y, D2*y are formed once per row.
+            float ek[G][9];  // A, C1, D1, P, Q, R, S, T, U
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                const ExactSlot &sl = my_slots[g];
+                ek[g][0] = fm[g].A; ek[g][1] = fm[g].C1; ek[g][2] = fm[g].D1;
+                ek[g][3] = sl.P; ek[g][4] = sl.Q; ek[g][5] = sl.R; ek[g][6] = sl.S; ek[g][7] = sl.T; ek[g][8] = sl.U;
+            }
+            int xx = pstart, yy = 0;
+            while (xx >= fw) { xx -= fw; yy++; }
+            float xf = (float)xx;
+            float eb[G][3];
+            auto set_row_e = [&](int yrow) {
+                const float yf = (float)(r0 + yrow);
 #pragma unroll
                 for (int g = 0; g < G; g++) {
                     const ExactSlot &sl = my_slots[g];
-                    ek[g][0] = fm[g].A; ek[g][1] = fm[g].C1; ek[g][2] = fm[g].D1;
-                    ek[g][3] = sl.P; ek[g][4] = sl.Q; ek[g][5] = sl.R; ek[g][6] = sl.S; ek[g][7] = sl.T; ek[g][8] = sl.U;
+                    eb[g][0] = xm(sl.B, yf);
+                    eb[g][1] = xm(sl.C2, yf);
+                    eb[g][2] = xm(sl.D2, yf);
                 }
-                int xx = lane, yy = 0;
-                while (xx >= fw) { xx -= fw; yy++; }
-                float xf = (float)xx;
-                float eb[G][3];
-                auto set_row_e = [&](int yrow) {
-                    const float yf = (float)(r0 + yrow);
+            };
+            set_row_e(yy);
+            while (yy < rows) {
+                FixTerms ft[C];
 #pragma unroll
-                    for (int g = 0; g < G; g++) {
-                        const ExactSlot &sl = my_slots[g];
-                        eb[g][0] = xm(sl.B, yf);
-                        eb[g][1] = xm(sl.C2, yf);
-                        eb[g][2] = xm(sl.D2, yf);
+                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B);
+                float ex[G], ey[G];
+                bool ins[G];
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const float w = xs(xa(xa(xm(ek[g][0], xf), eb[g][0]), ek[g][3]), ek[g][4]);
+                    const float X = xs(xa(xa(xm(ek[g][1], xf), eb[g][1]), ek[g][5]), ek[g][6]);
+                    const float Y = xs(xa(xa(xm(ek[g][2], xf), eb[g][2]), ek[g][7]), ek[g][8]);
+                    ex[g] = xd(X, w);
+                    ey[g] = xd(Y, w);
+                    ins[g] = in_image(ey[g], ex[g], mov_wf, mov_hf);
+                }
+                float v[G][C];
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const float fx = ins[g] ? floorf(ex[g]) : 0.0f, fy = ins[g] ? floorf(ey[g]) : 0.0f;
+                    const float ax = xs(ex[g], fx), ay = xs(ey[g], fy);
+                    const float omx = xs(1.0f, ax), omy = xs(1.0f, ay);
+                    const float u = ins[g] ? fx + 1.0f : -4.0f;
+                    const int base = (int)fx + mpitch * (int)fy;
+#pragma unroll
+                    for (int c = 0; c < C; c++) {
+                        float v00, v01, v10, v11;
+                        if constexpr (kTexTaps) {
+                            const float4 t4 = tex2Dgather<float4>(mtex, u, fy + 1.0f + (float)c * mrows, 0);
+                            v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
+                        } else {
+                            const float *pl = mdata + c * mplane + base;
+                            v00 = __ldg(pl); v01 = __ldg(pl + 1);
+                            v10 = __ldg(pl + mpitch); v11 = __ldg(pl + mpitch + 1);
+                        }
+                        const float top = xa(xm(omx, v00), xm(ax, v01));
+                        const float bot = xa(xm(omx, v10), xm(ax, v11));
+                        v[g][c] = ins[g] ? xa(xm(omy, top), xm(ay, bot)) : 0.0f;
                     }
-                };
-                set_row_e(yy);
-                while (yy < rows) {
-                    FixTerms ft[C];
+                }
 #pragma unroll
-                    for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], p);
-                    float ex[G], ey[G];
-                    bool ins[G];
-#pragma unroll
-                    for (int g = 0; g < G; g++) {
-                        const float w = xs(xa(xa(xm(ek[g][0], xf), eb[g][0]), ek[g][3]), ek[g][4]);
-                        const float X = xs(xa(xa(xm(ek[g][1], xf), eb[g][1]), ek[g][5]), ek[g][6]);
-                        const float Y = xs(xa(xa(xm(ek[g][2], xf), eb[g][2]), ek[g][7]), ek[g][8]);
-                        ex[g] = xd(X, w);
-                        ey[g] = xd(Y, w);
-                        ins[g] = in_image(ey[g], ex[g], p.mov_wf, p.mov_hf);
-                    }
-                    float v[G][C];
-#pragma unroll
-                    for (int g = 0; g < G; g++) {
-                        const float fx = ins[g] ? floorf(ex[g]) : 0.0f, fy = ins[g] ? floorf(ey[g]) : 0.0f;
-                        const float ax = xs(ex[g], fx), ay = xs(ey[g], fy);
-                        const float omx = xs(1.0f, ax), omy = xs(1.0f, ay);
-                        const float u = ins[g] ? fx + 1.0f : -4.0f;
-                        const int base = (int)fx + mpitch * (int)fy;
+                for (int g = 0; g < G; g++) {
+                    if (ins[g] || kAllPixels) {
 #pragma unroll
                         for (int c = 0; c < C; c++) {
-                            float v00, v01, v10, v11;
-                            if constexpr (kTexTaps) {
-                                const float4 t4 = tex2Dgather<float4>(p.mov_tex, u, fy + 1.0f + (float)c * mrows, 0);
-                                v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
+                            if constexpr (kMI) {
+                                const int bm = min(max((int)floorf(v[g][c] * sB), 0), B - 1);
+                                atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
                             } else {
-                                const float *pl = mdata + c * mplane + base;
-                                v00 = __ldg(pl); v01 = __ldg(pl + 1);
-                                v10 = __ldg(pl + mpitch); v11 = __ldg(pl + mpitch + 1);
+                                accumulate<COST>(part[g], ft[c], v[g][c]);
                             }
-                            const float top = xa(xm(omx, v00), xm(ax, v01));
-                            const float bot = xa(xm(omx, v10), xm(ax, v11));
-                            v[g][c] = ins[g] ? xa(xm(omy, top), xm(ay, bot)) : 0.0f;
                         }
-                    }
-#pragma unroll
-                    for (int g = 0; g < G; g++) {
-                        if (ins[g] || kAllPixels) {
-#pragma unroll
-                            for (int c = 0; c < C; c++) {
-                                if constexpr (kMI) {
-                                    const int bm = min(max((int)floorf(v[g][c] * sB), 0), B - 1);
-                                    atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
-                                } else {
-                                    accumulate<COST>(part[g], ft[c], v[g][c]);
-                                }
-                            }
-                            cnt[g] += C;
-                        }
-                    }
-                    xx += 32;
-                    xf += 32.0f;
-                    if (xx >= fw) {
-                        do { xx -= fw; yy++; } while (xx >= fw);
-                        xf = (float)xx;
-                        if (yy < rows) set_row_e(yy);
+                        cnt[g] += C;
                     }
                 }
-            } else {
-            int xx = lane, yy = 0;
+                xx += PSTEP;
+                xf += (float)PSTEP;
+                if (xx >= fw) {
+                    do { xx -= fw; yy++; } while (xx >= fw);
+                    xf = (float)xx;
+                    if (yy < rows) set_row_e(yy);
+                }
+            }
+        } else {
+            int xx = pstart, yy = 0;
             while (xx >= fw) { xx -= fw; yy++; }
             float xf = (float)xx;
             float byw[G], byx[G], byy[G];
@@ -597,7 +639,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
             while (yy < rows) {
                 FixTerms ft[C];
 #pragma unroll
-                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], p);
+                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B);
                 // 1. fast coordinates and decisions of all G points (independent chains)
                 bool fin[G], amb[G];
                 float mxs[G], mys[G];
@@ -629,7 +671,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                     for (int c = 0; c < C; c++) {
                         float v00, v01, v10, v11;
                         if constexpr (kTexTaps) {
-                            const float4 t4 = tex2Dgather<float4>(p.mov_tex, u, fy + 1.0f + (float)c * mrows, 0);
+                            const float4 t4 = tex2Dgather<float4>(mtex, u, fy + 1.0f + (float)c * mrows, 0);
                             // gather order: x = (i0, j1), y = (i1, j1), z = (i1, j0), w = (i0, j0)
                             v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
                         } else {
@@ -670,7 +712,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                                              fm[g].D1, sl.D2, sl.T, sl.U};
                             float ex, ey;
                             exact_map(kc, xf, (float)(r0 + yy), ex, ey);
-                            if (in_image(ey, ex, p.mov_wf, p.mov_hf)) {
+                            if (in_image(ey, ex, mov_wf, mov_hf)) {
                                 fin[g] = true;
 #pragma unroll
                                 for (int c = 0; c < C; c++) v[g][c] = bilinear_in(mdata + c * mplane, mpitch, ey, ex);
@@ -698,32 +740,61 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                         cnt[g] += C;
                     }
                 }
-                xx += 32;
-                xf += 32.0f;
+                xx += PSTEP;
+                xf += (float)PSTEP;
                 if (xx >= fw) {
                     do { xx -= fw; yy++; } while (xx >= fw);
                     xf = (float)xx;
                     if (yy < rows) set_row(yy);
                 }
             }
-            }  // fast sampling
-            if constexpr (!kMI) {
+        }  // fast sampling
+        if constexpr (!kMI) {
 #pragma unroll
-                for (int g = 0; g < G; g++)
+            for (int g = 0; g < G; g++)
 #pragma unroll
-                    for (int j = 0; j < NA; j++) tot[(g * NA + j) * 32] += part[g][j];
-            }
-
-            __syncthreads();
-            if (*abort_flag) {
-                aborted = true;
-                break;
-            }
-            if (threadIdx.x == 0 && it + kStages < total_it) issue(it + kStages);
+                for (int j = 0; j < NA; j++) tot[(g * NA + j) * 32] += part[g][j];
         }
-        if (aborted) break;
 
-        // ---- per grid point: reduce, finalise, dump, argmin ----
+        __syncthreads();
+        if (*sm.abort_flag) return false;
+        if (threadIdx.x == 0) prod.after_chunk(it);
+    }
+
+    // ---- per grid point: reduce, finalise, dump, argmin key ----
+    // Final MI cost of histogram h (B x B counts plus a marginal row and column) over n terms;
+    // one warp.
+    auto mi_cost = [&](uint32_t *h, int n) -> float {
+        // marginals: fixed (row sums) into column B, moving (column sums) into row B
+        for (int i = lane; i < B; i += 32) {
+            uint32_t rs = 0, cs = 0;
+            for (int j = 0; j < B; j++) {
+                rs += h[i * hstride + j];
+                cs += h[j * hstride + i];
+            }
+            h[i * hstride + B] = rs;
+            h[B * hstride + i] = cs;
+        }
+        __syncwarp();
+        const float nf = (float)n;
+        float s = 0.0f;
+        for (int j = lane; j < B; j += 32) {
+            const float hm = (float)h[B * hstride + j];
+            for (int i = 0; i < B; i++) {
+                const uint32_t v = h[i * hstride + j];
+                if (v) {
+                    const float vf = (float)v;
+                    const float hf = (float)h[i * hstride + B];
+                    s += vf * log2f((vf * nf) / (hf * hm));
+                }
+            }
+        }
+        s = warp_sum(s);
+        return (n == 0 || nf < p.gate_n) ? __int_as_float(0x7f800000) : -s / p.total_terms;
+    };
+
+    unsigned long long kk = ~0ull;
+    if constexpr (!BSPLIT) {
         float my_cost = 0.0f;
 #pragma unroll
         for (int g = 0; g < G; g++) {
@@ -731,33 +802,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
             float cost;
             if constexpr (kMI) {
                 __syncwarp();
-                uint32_t *h = hist + g * hsize;
-                // marginals: fixed (row sums) into column B, moving (column sums) into row B
-                for (int i = lane; i < B; i += 32) {
-                    uint32_t rs = 0, cs = 0;
-                    for (int j = 0; j < B; j++) {
-                        rs += h[i * hstride + j];
-                        cs += h[j * hstride + i];
-                    }
-                    h[i * hstride + B] = rs;
-                    h[B * hstride + i] = cs;
-                }
-                __syncwarp();
-                const float nf = (float)n;
-                float s = 0.0f;
-                for (int j = lane; j < B; j += 32) {
-                    const float hm = (float)h[B * hstride + j];
-                    for (int i = 0; i < B; i++) {
-                        const uint32_t v = h[i * hstride + j];
-                        if (v) {
-                            const float vf = (float)v;
-                            const float hf = (float)h[i * hstride + B];
-                            s += vf * log2f((vf * nf) / (hf * hm));
-                        }
-                    }
-                }
-                s = warp_sum(s);
-                cost = (n == 0 || nf < p.gate_n) ? __int_as_float(0x7f800000) : -s / p.total_terms;
+                cost = mi_cost(hist + g * hsize, n);
             } else {
                 float a[NA];
 #pragma unroll
@@ -767,7 +812,6 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
             if (lane == g) my_cost = cost;
         }
         // lanes 0..G-1 hold the costs of the warp's points
-        unsigned long long kk = ~0ull;
         if (lane < G) {
             bool valid = false;
             uint32_t idx = 0;
@@ -779,24 +823,93 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
                 kk = make_key(my_cost, idx);
             }
         }
-        kk = warp_min_u64(kk);
-        best = kk < best ? kk : best;
-        __syncwarp();  // the slots and histograms are rewritten by the next task
+    } else {
+        // the warps' counts, then warp g (mod NW) finalises point g from every warp's sums
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int n = warp_sum_i(cnt[g]);
+            if (lane == 0) sm.cnts[warp * G + g] = n;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            if (g % NW != warp) continue;
+            int n = 0;
+            for (int w = 0; w < NW; w++) n += sm.cnts[w * G + g];
+            float cost;
+            if constexpr (kMI) {
+                cost = mi_cost(hist + g * hsize, n);
+            } else {
+                float a[NA];
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    float v = 0.0f;
+                    for (int w = 0; w < NW; w++) v += sm.acc[(w * G + g) * NA * 32 + j * 32 + lane];
+                    a[j] = warp_sum(v);
+                }
+                cost = finalize<COST>(a, n, p);
+            }
+            if (lane == 0 && gvalid[g]) {
+                if (p.costs) p.costs[gidx[g]] = cost;
+                const unsigned long long k = make_key(cost, gidx[g]);
+                kk = k < kk ? k : kk;
+            }
+        }
     }
-
-    // ---- CTA argmin, one atomic per CTA, last CTA writes the result ----
-    if (lane == 0) wbest[warp] = best;
-    __syncthreads();
+    kk = warp_min_u64(kk);
+    if (lane == 0) sm.wbest[warp] = kk;
+    __syncthreads();  // keys complete; slots, sums and histograms are free for the next task
     if (threadIdx.x == 0) {
         unsigned long long b = ~0ull;
-        for (int w = 0; w < NW; w++) b = wbest[w] < b ? wbest[w] : b;
-        if (b != ~0ull) atomicMin(p.key, b);
-        if (*abort_flag) atomicOr(p.status, (unsigned)CGS_ERROR_DEVICE_TIMEOUT);
-        __threadfence();
-        const unsigned int ticket = atomicAdd(p.done, 1u);
-        if (ticket == gridDim.x - 1) {
-            __threadfence();
-            write_result(p);
+        for (int w = 0; w < NW; w++) b = sm.wbest[w] < b ? sm.wbest[w] : b;
+        retire_tasks(p, b, 1u, false);
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------- the single-pair kernel
+
+// Producer of the single-pair kernel: the CTA's tasks are blockIdx.x + k * gridDim.x, each
+// with the pair's num_chunks chunks, so iteration `it` is chunk it % num_chunks.
+template <int C>
+struct StaticProducer {
+    const SearchParams *p;
+    const CtaSmem *sm;
+    uint32_t total_it;
+    __device__ __forceinline__ void issue(uint32_t it) {
+        issue_chunk<C>(*p, *sm, it, (int)(it % (uint32_t)p->num_chunks));
+    }
+    __device__ __forceinline__ void after_chunk(uint32_t it) {
+        if (it + kStages < total_it) issue(it + kStages);
+    }
+};
+
+// NW warps per CTA; 512 / (32 NW) CTAs share an SM (two CTAs of 8 warps hide each
+// other's chunk barriers).  Tasks are dealt round-robin over the persistent CTAs.
+template <int COST, int C, int G, int NW, bool TEX = (COST != CGS_COST_MI)>
+__global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_constant__ SearchParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const CtaSmem sm = carve_smem<G, NW>(smem, p.chunk_rows * p.fix.pitch * C);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) mbar_init(&sm.bars[s], 1);
+        fence_mbar_init();
+        *sm.abort_flag = 0;
+    }
+    __syncthreads();
+
+    const uint32_t my_tasks =
+        (p.num_tasks > blockIdx.x) ? (p.num_tasks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+    StaticProducer<C> prod{&p, &sm, my_tasks * (uint32_t)p.num_chunks};
+    if (threadIdx.x == 0) {
+        for (uint32_t it = 0; it < (uint32_t)kStages && it < prod.total_it; it++) prod.issue(it);
+    }
+
+    uint32_t it = 0;
+    for (uint32_t k = 0; k < my_tasks; k++) {
+        if (!run_task<COST, C, G, NW, TEX, false>(p, blockIdx.x + k * gridDim.x, sm, it, prod)) {
+            // a bounded wait gave up: retire this CTA's remaining tasks with the timeout status
+            if (threadIdx.x == 0) retire_tasks(p, ~0ull, my_tasks - k, true);
+            return;
         }
     }
 }

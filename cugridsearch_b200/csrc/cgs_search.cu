@@ -178,23 +178,6 @@ static void locality_order(int cost, const cgs_grid &g, int fw, int fh, int mw, 
 
 // ---------------------------------------------------------------- kernels: staging, argmin
 
-struct PrepParams {
-    const void *mov_src;
-    const void *fix_src;
-    int32_t mov_pix, fix_pix;
-    int32_t mh, mw, fh, fw, c;
-    float *mov_dst;
-    float *fix_dst;
-    int64_t mplane, fplane;
-    int32_t mpitch, fpitch;
-    unsigned long long *key;
-    unsigned int *done;
-    unsigned int *status;
-    float *vmax;  // zeroed before the launch
-    int32_t fix_alias;   // stage the fixed image like the moving one (scanline functors)
-    float *row_table;    // calcMIAlt row values, or null
-    int32_t rowsf;
-};
 
 __device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
     switch (pix) {
@@ -209,9 +192,7 @@ __device__ __forceinline__ float load_pix(const void *src, int pix, int64_t i) {
 // `mpitch` floats: pixels in columns 0..W-1, pixel (0, y + 1) in column W (the reference's
 // flat-index neighbour of (W - 1, y)), zeros elsewhere, a zero row H.  Fixed planes use a
 // 16-byte row pitch so rows can be bulk-copied.
-__global__ void prep_kernel(const PrepParams q) {
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+__device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int64_t nthr) {
     if (tid == 0) {
         *q.key = ~0ull;
         *q.done = 0u;
@@ -256,6 +237,17 @@ __global__ void prep_kernel(const PrepParams q) {
         }
     }
 }
+
+__global__ void prep_kernel(const PrepParams q) {
+    prep_body(q, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+// Staging of a batch: blockIdx.y selects the pair, the x blocks stride over its elements.
+__global__ void batch_prep_kernel(const PrepParams *__restrict__ qs) {
+    prep_body(qs[blockIdx.y], blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+const void *batch_prep_kernel_fn() { return (const void *)batch_prep_kernel; }
 
 __global__ void empty_result_kernel(cgs_argmin *r) {
     cgs_argmin e;
@@ -347,15 +339,9 @@ __global__ void hist_kernel(const HistParams hp) {
 
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
-// Staged layout of a moving/fixed image pair inside one scratch block.
-struct Staging {
-    int32_t mpitch = 0, fpitch = 0;
-    int64_t mplane = 0, fplane = 0;
-    size_t mov_off = 0, fix_off = 0, rows_off = 0, bytes = 0;
-};
 
 // Sampling mode of a request (see CGS_FLAG_EXACT_SAMPLES / CGS_FLAG_FAST_SAMPLES).
-static bool exact_samples(int cost, int flags) {
+bool exact_samples(int cost, int flags) {
     if (flags & CGS_FLAG_EXACT_SAMPLES) return true;
     if (flags & CGS_FLAG_FAST_SAMPLES) return false;
     return !(cost == CGS_COST_ZNCC || cost == CGS_COST_MI);
@@ -377,8 +363,8 @@ static int32_t mi_alt_rows(int rowsf) {
     return n;
 }
 
-static Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align,
-                              bool fix_alias = false, bool row_table = false) {
+Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align,
+                              bool fix_alias, bool row_table) {
     Staging st;
     const int C = fix.channels;
     st.mpitch = (int32_t)round_up(mov.width + 1, std::max(1, tex_pitch_align / 4));
@@ -394,7 +380,7 @@ static Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int te
 }
 
 // Origin of a staging block: the first tex_align boundary at or after the allocation.
-static char *staging_origin(void *scratch, int tex_align) {
+char *staging_origin(void *scratch, int tex_align) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(scratch);
     return reinterpret_cast<char *>((a + (uintptr_t)tex_align - 1) / (uintptr_t)tex_align * (uintptr_t)tex_align);
 }
@@ -498,6 +484,114 @@ cgs_status check_grid(const cgs_grid *g) {
     return CGS_SUCCESS;
 }
 
+// Validates a search request (images, grid, options) as cgs_search does; *mi_bins gets the
+// MI bin count in use.
+cgs_status check_request(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options *options,
+                         int *mi_bins) {
+    cgs_status s;
+    if ((s = check_image(mov, "moving")) != CGS_SUCCESS) return s;
+    if ((s = check_image(fix, "fixed")) != CGS_SUCCESS) return s;
+    if ((s = check_grid(grid)) != CGS_SUCCESS) return s;
+    if (!options) return fail(CGS_ERROR_INVALID_VALUE, "options is null");
+    const int cost = options->cost;
+    if (cost < 0 || cost >= CGS_COST_COUNT) return fail(CGS_ERROR_INVALID_VALUE, "unknown cost");
+    if (mov->channels != fix->channels)
+        return fail(CGS_ERROR_INVALID_VALUE, "moving and fixed images must have the same channel count");
+    const bool eight = !(cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF);
+    if (eight && grid->dims != 8) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs an 8-parameter grid");
+    if (!eight && grid->dims < 2) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs a grid of >= 2 axes");
+    if ((cost == CGS_COST_SAD_AVG_H || cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF) &&
+        fix->channels != 1)
+        return fail(CGS_ERROR_INVALID_VALUE, "this reference functor is single-channel (CudaImage<T>)");
+    *mi_bins = 32;
+    if (cost == CGS_COST_MI) {
+        *mi_bins = options->mi_bins == 0 ? 32 : options->mi_bins;
+        if (*mi_bins < 2 || *mi_bins > 64 || (*mi_bins & (*mi_bins - 1)))
+            return fail(CGS_ERROR_INVALID_VALUE, "mi_bins must be a power of two in [2, 64]");
+    }
+    return CGS_SUCCESS;
+}
+
+// Kernel parameters of a validated pixel-loop request, except the staged planes, scratch
+// words, outputs and texture: the reference's grid tables, the evaluation order, cos/sin of
+// the rotation axis, image geometry and cost options.  *n64 = grid points.
+cgs_status fill_params(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options &o,
+                       int mi_bins, SearchParams *pp, int64_t *n64) {
+    const int cost = o.cost;
+    const int C = fix->channels;
+    int32_t inc[8];
+    grid_increments(*grid, inc, n64);
+    if (*n64 > INT32_MAX) return fail(CGS_ERROR_GRID_TOO_LARGE, "grid has more than 2^31-1 points");
+    SearchParams &p = *pp;
+    memset(&p, 0, sizeof(p));
+    if (*n64 <= 0) return CGS_SUCCESS;
+    for (int a = 0; a < 8; a++) {
+        p.start[a] = a < grid->dims ? grid->start[a] : 0.0f;
+        p.res[a] = a < grid->dims ? grid->resolution[a] : 0.0f;
+        p.inc[a] = inc[a];
+    }
+    p.dims = grid->dims;
+    p.cost = cost;
+    p.n = (uint32_t)*n64;
+    p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
+    p.exact_only = exact_samples(cost, o.flags) ? 1 : 0;
+    if (!p.natural) {
+        locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
+        for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
+    }
+    if (cost_uses_theta(cost)) {
+        // cos/sin of every axis-0 grid value, with the host libm the reference's CPU path uses
+        const int32_t n0 = grid->dims > 1 ? inc[1] : (int32_t)*n64;
+        if (n0 > kMaxTrig) return fail(CGS_ERROR_UNSUPPORTED, "more than 256 values on the rotation axis");
+        for (int32_t i = 0; i < n0; i++) {
+            const float th = std::fmaf((float)i, grid->resolution[0], grid->start[0]);
+            p.trig[i] = make_float2(std::cos(th), std::sin(th));
+        }
+    }
+    p.mov_wf = (float)mov->width;
+    p.mov_hf = (float)mov->height;
+    p.cx = (float)mov->width / 2;
+    p.cy = (float)mov->height / 2;
+    p.mi_bins = mi_bins;
+    p.total_terms = (float)((double)fix->width * fix->height * C);
+    p.gate_n = (float)((double)o.overlap_gate * fix->width * fix->height * C);
+    return CGS_SUCCESS;
+}
+
+// Fixed-image chunking: about 16 KB of rows per chunk (at least one row).  Returns the bytes
+// of one stage.
+int64_t set_chunks(SearchParams *p, const Staging &st, int C, int fix_h) {
+    const int64_t row_bytes = (int64_t)st.fpitch * 4 * C;
+    int R = (int)std::max<int64_t>(1, 16384 / row_bytes);
+    R = std::min(R, fix_h);
+    p->chunk_rows = R;
+    p->num_chunks = (fix_h + R - 1) / R;
+    return (int64_t)R * row_bytes;
+}
+
+// Staging-kernel parameters of a pair whose scratch words start at sb (key, done, status,
+// max |moving pixel|) and whose staged planes are at mstage / fstage.
+PrepParams make_prep(const cgs_image *mov, const cgs_image *fix, const Staging &st, char *sb, float *mstage,
+                     float *fstage) {
+    PrepParams q{};  // every field zero unless set below
+    q.mov_src = mov->data;
+    q.fix_src = fix->data;
+    q.mov_pix = mov->pixel;
+    q.fix_pix = fix->pixel;
+    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = fix->channels;
+    q.mov_dst = mstage;
+    q.fix_dst = fstage;
+    q.mplane = st.mplane;
+    q.fplane = st.fplane;
+    q.mpitch = st.mpitch;
+    q.fpitch = st.fpitch;
+    q.key = reinterpret_cast<unsigned long long *>(sb);
+    q.done = reinterpret_cast<unsigned int *>(sb + 8);
+    q.status = reinterpret_cast<unsigned int *>(sb + 12);
+    q.vmax = reinterpret_cast<float *>(sb + 16);
+    return q;
+}
+
 struct Plan {
     int G = 2, NW = 16;
 };
@@ -509,6 +603,12 @@ static int accumulators(int cost) {
         case CGS_COST_ZNCC: return AccN<CGS_COST_ZNCC>::value;
         default: return 1;
     }
+}
+
+// Bytes of a CTA's sums or MI histograms region (CtaSmem::acc).
+size_t acc_bytes(int cost, int G, int NW, bool block_split, int mi_bins) {
+    if (cost == CGS_COST_MI) return (size_t)(block_split ? 1 : NW) * G * (mi_bins + 1) * (mi_bins + 1) * 4;
+    return (size_t)NW * G * accumulators(cost) * 32 * 4;
 }
 
 static Plan choose_plan(int cost, const cgs_options &o, int mi_bins) {
@@ -550,6 +650,7 @@ static cgs_status search_scanline(const cgs_image *mov, const cgs_image *fix, co
         p.inc[a] = inc[a];
     }
     p.dims = grid->dims;
+    p.cost = cost;
     p.n = (uint32_t)n64;
     p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
     if (!p.natural) {
@@ -714,28 +815,11 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
                       float *costs, cgs_argmin *result, cgs_stream_t stream_) {
     cudaStream_t stream = (cudaStream_t)stream_;
     cgs_status s;
-    if ((s = check_image(mov, "moving")) != CGS_SUCCESS) return s;
-    if ((s = check_image(fix, "fixed")) != CGS_SUCCESS) return s;
-    if ((s = check_grid(grid)) != CGS_SUCCESS) return s;
-    if (!options) return fail(CGS_ERROR_INVALID_VALUE, "options is null");
+    int mi_bins = 32;
+    if ((s = check_request(mov, fix, grid, options, &mi_bins)) != CGS_SUCCESS) return s;
     if (!result) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
     const cgs_options o = *options;
     const int cost = o.cost;
-    if (cost < 0 || cost >= CGS_COST_COUNT) return fail(CGS_ERROR_INVALID_VALUE, "unknown cost");
-    if (mov->channels != fix->channels)
-        return fail(CGS_ERROR_INVALID_VALUE, "moving and fixed images must have the same channel count");
-    const bool eight = !(cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF);
-    if (eight && grid->dims != 8) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs an 8-parameter grid");
-    if (!eight && grid->dims < 2) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs a grid of >= 2 axes");
-    if ((cost == CGS_COST_SAD_AVG_H || cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF) &&
-        fix->channels != 1)
-        return fail(CGS_ERROR_INVALID_VALUE, "this reference functor is single-channel (CudaImage<T>)");
-    int mi_bins = 32;
-    if (cost == CGS_COST_MI) {
-        mi_bins = o.mi_bins == 0 ? 32 : o.mi_bins;
-        if (mi_bins < 2 || mi_bins > 64 || (mi_bins & (mi_bins - 1)))
-            return fail(CGS_ERROR_INVALID_VALUE, "mi_bins must be a power of two in [2, 64]");
-    }
     if (is_scanline(cost)) {
         DeviceInfo dsi;
         if ((s = device_info(&dsi)) != CGS_SUCCESS) return s;
@@ -751,59 +835,19 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     DeviceInfo di;
     if ((s = device_info(&di)) != CGS_SUCCESS) return s;
 
-    int32_t inc[8];
+    SearchParams p;
     int64_t n64;
-    grid_increments(*grid, inc, &n64);
-    if (n64 > INT32_MAX) return fail(CGS_ERROR_GRID_TOO_LARGE, "grid has more than 2^31-1 points");
+    if ((s = fill_params(mov, fix, grid, o, mi_bins, &p, &n64)) != CGS_SUCCESS) return s;
     if (n64 <= 0) {
         empty_result_kernel<<<1, 1, 0, stream>>>(result);
         CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
         return CGS_SUCCESS;
     }
 
-    SearchParams p;
-    memset(&p, 0, sizeof(p));
-    for (int a = 0; a < 8; a++) {
-        p.start[a] = a < grid->dims ? grid->start[a] : 0.0f;
-        p.res[a] = a < grid->dims ? grid->resolution[a] : 0.0f;
-        p.inc[a] = inc[a];
-    }
-    p.dims = grid->dims;
-    p.n = (uint32_t)n64;
-    p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
-    p.exact_only = exact_samples(cost, o.flags) ? 1 : 0;
-    if (!p.natural) {
-        locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
-        for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
-    }
-    if (cost_uses_theta(cost)) {
-        // cos/sin of every axis-0 grid value, with the host libm the reference's CPU path uses
-        const int32_t n0 = grid->dims > 1 ? inc[1] : (int32_t)n64;
-        if (n0 > kMaxTrig) return fail(CGS_ERROR_UNSUPPORTED, "more than 256 values on the rotation axis");
-        for (int32_t i = 0; i < n0; i++) {
-            const float th = std::fmaf((float)i, grid->resolution[0], grid->start[0]);
-            p.trig[i] = make_float2(std::cos(th), std::sin(th));
-        }
-    }
-    p.mov_wf = (float)mov->width;
-    p.mov_hf = (float)mov->height;
-    p.cx = (float)mov->width / 2;
-    p.cy = (float)mov->height / 2;
-    p.mi_bins = mi_bins;
-    p.total_terms = (float)((double)fix->width * fix->height * C);
-    p.gate_n = (float)((double)o.overlap_gate * fix->width * fix->height * C);
-
     // staged layout
     const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align);
-    const int64_t row_bytes = (int64_t)st.fpitch * 4 * C;
-    int R = (int)std::max<int64_t>(1, 16384 / row_bytes);
-    R = std::min(R, fix->height);
-    p.chunk_rows = R;
-    p.num_chunks = (fix->height + R - 1) / R;
-    const int64_t stage_bytes = (int64_t)R * row_bytes;
-    size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes + (size_t)pl.NW * pl.G * sizeof(ExactSlot);
-    if (cost == CGS_COST_MI) smem += (size_t)pl.NW * pl.G * (mi_bins + 1) * (mi_bins + 1) * 4;
-    else smem += (size_t)pl.NW * pl.G * accumulators(cost) * 32 * 4;
+    const int64_t stage_bytes = set_chunks(&p, st, C, fix->height);
+    const size_t smem = cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes, acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
 
     cudaMemPool_t pool;
@@ -822,22 +866,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.costs = costs;
     p.result = result;
 
-    PrepParams q{};  // every field zero unless set below
-    q.mov_src = mov->data;
-    q.fix_src = fix->data;
-    q.mov_pix = mov->pixel;
-    q.fix_pix = fix->pixel;
-    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
-    q.mov_dst = mstage;
-    q.fix_dst = fstage;
-    q.mplane = st.mplane;
-    q.fplane = st.fplane;
-    q.mpitch = st.mpitch;
-    q.fpitch = st.fpitch;
-    q.key = p.key;
-    q.done = p.done;
-    q.status = p.status;
-    q.vmax = reinterpret_cast<float *>(sb + 16);
+    PrepParams q = make_prep(mov, fix, st, sb, mstage, fstage);
     const int64_t prep_elems = (st.mplane + st.fplane) * C;
     const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
     cudaError_t e = cudaMemsetAsync(sb, 0, 256, stream);
@@ -963,28 +992,11 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
                               const cgs_options *options, float *costs, cgs_argmin *result, cgs_stream_t stream_) {
     cudaStream_t stream = (cudaStream_t)stream_;
     cgs_status s;
-    if ((s = check_image(mov, "moving")) != CGS_SUCCESS) return s;
-    if ((s = check_image(fix, "fixed")) != CGS_SUCCESS) return s;
-    if ((s = check_grid(grid)) != CGS_SUCCESS) return s;
-    if (!options) return fail(CGS_ERROR_INVALID_VALUE, "options is null");
+    int mi_bins = 32;
+    if ((s = check_request(mov, fix, grid, options, &mi_bins)) != CGS_SUCCESS) return s;
     if (!result) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
     const cgs_options o = *options;
     const int cost = o.cost;
-    if (cost < 0 || cost >= CGS_COST_COUNT) return fail(CGS_ERROR_INVALID_VALUE, "unknown cost");
-    if (mov->channels != fix->channels)
-        return fail(CGS_ERROR_INVALID_VALUE, "moving and fixed images must have the same channel count");
-    const bool eight = !(cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF);
-    if (eight && grid->dims != 8) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs an 8-parameter grid");
-    if (!eight && grid->dims < 2) return fail(CGS_ERROR_INVALID_VALUE, "this cost needs a grid of >= 2 axes");
-    if ((cost == CGS_COST_SAD_AVG_H || cost == CGS_COST_SAD_SUM_T || cost == CGS_COST_SAD_SUM_T_REF) &&
-        fix->channels != 1)
-        return fail(CGS_ERROR_INVALID_VALUE, "this reference functor is single-channel (CudaImage<T>)");
-    int mi_bins = 32;
-    if (cost == CGS_COST_MI) {
-        mi_bins = o.mi_bins == 0 ? 32 : o.mi_bins;
-        if (mi_bins < 2 || mi_bins > 64 || (mi_bins & (mi_bins - 1)))
-            return fail(CGS_ERROR_INVALID_VALUE, "mi_bins must be a power of two in [2, 64]");
-    }
     const int C = fix->channels;
     // fixed tuning: the plan's MI shape, else 4 points per warp and 16 warps per CTA
     Plan pl;
@@ -1012,56 +1024,17 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
     char *scratch = nullptr;
     if ((s = static_scratch(di.dev, &scratch)) != CGS_SUCCESS) return s;
 
-    int32_t inc[8];
+    SearchParams p;
     int64_t n64;
-    grid_increments(*grid, inc, &n64);
-    if (n64 > INT32_MAX) return fail(CGS_ERROR_GRID_TOO_LARGE, "grid has more than 2^31-1 points");
+    if ((s = fill_params(mov, fix, grid, o, mi_bins, &p, &n64)) != CGS_SUCCESS) return s;
     if (n64 <= 0) {
         empty_result_kernel<<<1, 1, 0, stream>>>(result);
         CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
         return CGS_SUCCESS;
     }
 
-    SearchParams p;
-    memset(&p, 0, sizeof(p));
-    for (int a = 0; a < 8; a++) {
-        p.start[a] = a < grid->dims ? grid->start[a] : 0.0f;
-        p.res[a] = a < grid->dims ? grid->resolution[a] : 0.0f;
-        p.inc[a] = inc[a];
-    }
-    p.dims = grid->dims;
-    p.n = (uint32_t)n64;
-    p.natural = ((o.flags & CGS_FLAG_NATURAL_ORDER) || !integral_counts(*grid)) ? 1 : 0;
-    p.exact_only = exact_samples(cost, o.flags) ? 1 : 0;
-    if (!p.natural) {
-        locality_order(cost, *grid, fix->width, fix->height, mov->width, mov->height, p.perm);
-        for (int j = 0; j < grid->dims; j++) p.ocount[j] = (int32_t)grid->count[p.perm[j]];
-    }
-    if (cost_uses_theta(cost)) {
-        const int32_t n0 = grid->dims > 1 ? inc[1] : (int32_t)n64;
-        if (n0 > kMaxTrig) return fail(CGS_ERROR_UNSUPPORTED, "more than 256 values on the rotation axis");
-        for (int32_t i = 0; i < n0; i++) {
-            const float th = std::fmaf((float)i, grid->resolution[0], grid->start[0]);
-            p.trig[i] = make_float2(std::cos(th), std::sin(th));
-        }
-    }
-    p.mov_wf = (float)mov->width;
-    p.mov_hf = (float)mov->height;
-    p.cx = (float)mov->width / 2;
-    p.cy = (float)mov->height / 2;
-    p.mi_bins = mi_bins;
-    p.total_terms = (float)((double)fix->width * fix->height * C);
-    p.gate_n = (float)((double)o.overlap_gate * fix->width * fix->height * C);
-
-    const int64_t row_bytes = (int64_t)st.fpitch * 4 * C;
-    int R = (int)std::max<int64_t>(1, 16384 / row_bytes);
-    R = std::min(R, fix->height);
-    p.chunk_rows = R;
-    p.num_chunks = (fix->height + R - 1) / R;
-    const int64_t stage_bytes = (int64_t)R * row_bytes;
-    size_t smem = 128 + 8 * pl.NW + 2 * stage_bytes + (size_t)pl.NW * pl.G * sizeof(ExactSlot);
-    if (cost == CGS_COST_MI) smem += (size_t)pl.NW * pl.G * (mi_bins + 1) * (mi_bins + 1) * 4;
-    else smem += (size_t)pl.NW * pl.G * accumulators(cost) * 32 * 4;
+    const int64_t stage_bytes = set_chunks(&p, st, C, fix->height);
+    const size_t smem = cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes, acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
 
     // the static array is 256-byte aligned: the staging origin is its start
@@ -1078,22 +1051,7 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
     p.result = result;
     p.mov_tex = 0;  // the plain-load kernels read no texture
 
-    PrepParams q{};  // every field zero unless set below
-    q.mov_src = mov->data;
-    q.fix_src = fix->data;
-    q.mov_pix = mov->pixel;
-    q.fix_pix = fix->pixel;
-    q.mh = mov->height; q.mw = mov->width; q.fh = fix->height; q.fw = fix->width; q.c = C;
-    q.mov_dst = mstage;
-    q.fix_dst = fstage;
-    q.mplane = st.mplane;
-    q.fplane = st.fplane;
-    q.mpitch = st.mpitch;
-    q.fpitch = st.fpitch;
-    q.key = p.key;
-    q.done = p.done;
-    q.status = p.status;
-    q.vmax = reinterpret_cast<float *>(sb + 16);
+    PrepParams q = make_prep(mov, fix, st, sb, mstage, fstage);
     // the array keeps the previous call's contents: the header (argmin key, completion
     // counter, status, max |pixel|) is cleared here and the staging kernel rewrites every
     // staged element

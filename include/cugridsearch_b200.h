@@ -182,6 +182,81 @@ cgs_status cgs_covariance(const cgs_grid *grid, const float *costs, uint64_t n, 
 cgs_status cgs_mi_histogram(const cgs_image *moving, const cgs_image *fixed, const float params[8], int32_t bins,
                             uint32_t *hist, cgs_stream_t stream);
 
+/* ---------------------------------------------------------------- batched search
+ *
+ * Many image pairs of uneven sizes, each with its own grid and cost, evaluated by ONE
+ * persistent sm_100a launch.  The reference searches one pair per call and its callers loop
+ * over pairs and refinement levels (src/gpu/cudaGridSearch_main_mi.cu:312-363, one
+ * search_by_value + find_extrema per pass); a batch replaces that loop.  Each pair's costs and
+ * argmin equal those of cgs_search on the same pair: bit for bit with block_split = 0, within
+ * FP32 summation order with block_split = 1 (the argmin may then differ only between points
+ * whose costs tie within that rounding). */
+typedef struct cgs_pair {
+    cgs_image moving;      /* DEVICE images, single channel                                  */
+    cgs_image fixed;
+    cgs_grid grid;
+    cgs_options options;   /* cost: CGS_COST_SAD_AVG, _SQD_REF, _NCC_REF, _ZNCC or _MI; mi_bins,
+                              overlap_gate and flags as for cgs_search.  points_per_warp and
+                              warps_per_block are ignored: the batch plan applies            */
+    float *costs;          /* nullable DEVICE dump of this pair's grid (as cgs_search)       */
+    cgs_argmin *result;    /* DEVICE result of this pair                                     */
+} cgs_pair;
+
+/* Launch plan of the batch kernel (one for the whole launch). */
+typedef struct cgs_batch_plan {
+    int32_t points_per_warp; /* 1, 2, 4 or 8 grid points evaluated together by a warp          */
+    int32_t warps_per_block; /* 4, 8 or 16: blocks of 128, 256 or 512 threads                 */
+    int32_t block_split;     /* 0: each warp owns its points and sweeps every pixel for them; MI
+                                histograms are private per warp.  1: a block's warps share its
+                                points and split the pixels; MI histograms are per block      */
+    int32_t reserved;
+} cgs_batch_plan;
+
+/* One autotuner measurement: the plan, the kernel time on the tuning sample (+inf when the
+ * plan does not fit), and the status of the attempt. */
+typedef struct cgs_tune_entry {
+    cgs_batch_plan plan;
+    float ms;
+    int32_t status;
+} cgs_tune_entry;
+
+typedef struct cgs_batch cgs_batch; /* opaque handle */
+
+/* Creates a batch: validates every pair, lays out device scratch for all of them (one
+ * allocation, held until cgs_batch_destroy), orders the pairs by estimated work (cheapest
+ * first) and records one CUDA graph -- clear scratch, stage every pair, the persistent batch
+ * kernel -- for the plan (NULL: 2 points per warp, 16 warps, warp-private histograms, or
+ * block-shared ones where those do not fit).  The images, dumps and results are bound to the
+ * handle: update image CONTENTS in place between launches.  Errors name the failing pair. */
+cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_plan *plan, cgs_batch **batch);
+
+/* Replays the batch graph on `stream` (asynchronous).  Launches of one batch are serialised. */
+cgs_status cgs_batch_launch(cgs_batch *batch, cgs_stream_t stream);
+
+/* Sets the launch plan (re-records the graph) / reads it. */
+cgs_status cgs_batch_set_plan(cgs_batch *batch, const cgs_batch_plan *plan);
+cgs_status cgs_batch_get_plan(const cgs_batch *batch, cgs_batch_plan *plan);
+
+/* Autotuner: times every plan (points_per_warp x warps_per_block x block_split, 24 candidates)
+ * on a sample of the batch -- the first sample_points points of every pair's grid (<= 0: 4096),
+ * the kernel alone, best of two runs after a warm-up -- and applies the fastest.  entries (up to
+ * max_entries, nullable) receive every measurement. */
+cgs_status cgs_batch_autotune(cgs_batch *batch, int32_t sample_points, cgs_tune_entry *entries, int32_t max_entries,
+                              int32_t *n_entries, cgs_batch_plan *best);
+
+/* Device time stamps (%globaltimer, ns) of the last launch, per pair in the caller's order: the
+ * start of the pair's first task and the end of its last.  Waits for the launch. */
+cgs_status cgs_batch_pair_times(cgs_batch *batch, uint64_t *start_ns, uint64_t *end_ns);
+
+/* Releases the handle's graph, textures and device memory (waits for its last launch). */
+cgs_status cgs_batch_destroy(cgs_batch *batch);
+
+/* One-shot batch: create, launch on `stream`, wait, destroy.  Synchronous. */
+cgs_status cgs_search_batched(const cgs_pair *pairs, int32_t n, const cgs_batch_plan *plan, cgs_stream_t stream);
+
+/* Autotunes a temporary batch of these pairs and returns the best plan. */
+cgs_status cgs_autotune(const cgs_pair *pairs, int32_t n, int32_t sample_points, cgs_batch_plan *best);
+
 /* Synchronous convenience: cgs_search on `stream`, then copies the argmin to *host_result. */
 cgs_status cgs_search_sync(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
                            const cgs_options *options, float *costs, cgs_argmin *host_result,

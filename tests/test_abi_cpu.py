@@ -102,3 +102,50 @@ def test_python_mirror_rejects_host_memory():
     import cugridsearch_b200 as cgs
     with pytest.raises(TypeError):
         cgs.CudaImage(torch.from_numpy(np.zeros((4, 4), np.float32)))
+
+
+def test_batch_arguments_fail_before_device_work(lib):
+    """cgs_batch_create validates every pair (naming it) before touching the device."""
+    import cugridsearch_b200._abi as abi
+    L = lib
+    h = C.c_void_p(None)
+    assert L.cgs_batch_create(None, 0, None, C.byref(h)) == 1 and not h.value
+    g = abi.CgsGrid()
+    g.dims = 8
+    for a in range(8):
+        g.count[a] = 2.0
+        g.end[a] = 1.0
+    L.cgs_grid_update(C.byref(g), -1)
+    img = abi.CgsImage(16, 8, 8, 1, 0)
+    ok = abi.CgsOptions(abi.COSTS["ZNCC"], 0, 0.0, 0, 0, 0)
+
+    def pairs(*ps):
+        return (abi.CgsPair * len(ps))(*ps)
+
+    good = abi.CgsPair(img, img, g, ok, None, 64)
+    assert L.cgs_batch_create(pairs(good, abi.CgsPair(img, img, g, ok, None, None)), 2, None, C.byref(h)) == 1
+    assert b"pair 1" in L.cgs_last_error() and b"result" in L.cgs_last_error()
+    unsupported = abi.CgsOptions(abi.COSTS["SAD_AVG_H"], 0, 0.0, 0, 0, 0)
+    assert L.cgs_batch_create(pairs(abi.CgsPair(img, img, g, unsupported, None, 64)), 1, None, C.byref(h)) == 2
+    rgb = abi.CgsImage(16, 8, 8, 3, 0)
+    assert L.cgs_batch_create(pairs(abi.CgsPair(rgb, rgb, g, ok, None, 64)), 1, None, C.byref(h)) == 2
+    bad_bins = abi.CgsOptions(abi.COSTS["MI"], 48, 0.0, 0, 0, 0)
+    assert L.cgs_batch_create(pairs(abi.CgsPair(img, img, g, bad_bins, None, 64)), 1, None, C.byref(h)) == 1
+    assert not h.value
+
+
+def test_batch_struct_layout():
+    """The ctypes mirror of cgs_pair / cgs_batch_plan / cgs_tune_entry has the C sizes."""
+    import subprocess
+    import tempfile
+    import cugridsearch_b200._abi as abi
+    src = ('#include <stdio.h>\n#include <stddef.h>\n#include "cugridsearch_b200.h"\n'
+           'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(cgs_pair), offsetof(cgs_pair, costs),'
+           ' offsetof(cgs_pair, result), sizeof(cgs_batch_plan), sizeof(cgs_tune_entry)); return 0;}\n')
+    with tempfile.TemporaryDirectory() as d:
+        c_file, exe = os.path.join(d, "t.c"), os.path.join(d, "t")
+        open(c_file, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c_file, "-o", exe], check=True)
+        got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == [C.sizeof(abi.CgsPair), abi.CgsPair.costs.offset, abi.CgsPair.result.offset,
+                   C.sizeof(abi.CgsBatchPlan), C.sizeof(abi.CgsTuneEntry)]
