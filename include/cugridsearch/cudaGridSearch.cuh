@@ -369,13 +369,12 @@ struct FunctorList {
     typedef F (*Fn)(nv_ext::Vec<G, D> &, CudaImage<P, C>, CudaImage<P, C>);
     typedef KnownFunctor<F, G, D, P, C> Entry;
 
+    // The launcher is named in both compilation passes: the device pass instantiates
+    // direct_kernel<..., FN> only through it, and a launcher whose kernel has no device code
+    // fails at launch with "invalid device function".  On the device the pointer is never used.
     template <Fn FN>
     static CUDAFUNCTION Entry make(int cost, int bins) {
-#ifdef __CUDA_ARCH__
-        return Entry{reinterpret_cast<uintptr_t>(FN), cost, bins, nullptr};
-#else
         return Entry{reinterpret_cast<uintptr_t>(FN), cost, bins, &launch_direct<F, G, D, P, C, FN>};
-#endif
     }
 
     // Fills out (capacity 32); returns the count.  Device side: only addr is meaningful.

@@ -163,6 +163,7 @@ int main(int argc, char **argv) {
     std::ifstream list(in + "/cases.txt");
     std::string line;
     int done = 0;
+    std::string current;
     try {
         while (std::getline(list, line)) {
             if (line.empty() || line[0] == '#') continue;
@@ -177,6 +178,7 @@ int main(int argc, char **argv) {
             for (auto &v : cs.end) ss >> v;
             for (auto &v : cs.count) ss >> v;
             const std::string key = cs.pixel + ":" + std::to_string(cs.channels) + ":" + cs.functor;
+            current = cs.name;
             if (key == "f32:1:ncc") run<8, float, 1>(cs, fetch(d_f32_ncc), in, out);
             else if (key == "f32:1:sqd") run<8, float, 1>(cs, fetch(d_f32_sqd), in, out);
             else if (key == "f32:1:sad") run<8, float, 1>(cs, fetch(d_f32_sad), in, out);
@@ -207,7 +209,7 @@ int main(int argc, char **argv) {
             done++;
         }
     } catch (const cgs_compat::Error &e) {
-        fprintf(stderr, "error: %s\n", e.what());
+        fprintf(stderr, "error in case %s: %s\n", current.c_str(), e.what());
         return 1;
     }
     printf("%d cases\n", done);
