@@ -283,6 +283,8 @@ def main():
     ap.add_argument("--points-per-warp", type=int, default=0, help="0 = library choice")
     ap.add_argument("--ref-budget", type=float, default=6.0, help="seconds of CPU work per reference step")
     ap.add_argument("--small", action="store_true", help="3^8 grid (for profiling captures)")
+    ap.add_argument("--taps", default="auto", choices=["auto", "quad", "texture"],
+                    help="tap source of the fast path (auto: the library's choice)")
     ap.add_argument("--workload", default="ncc", choices=["ncc", "mi", "sad", "batch"],
                     help="ncc: the headline 256^2 ZNCC pair; mi: 512^2 u8 MI pair; sad: 64^2 SAD pair; "
                          "batch: 64 uneven pairs in one persistent launch")
@@ -333,7 +335,8 @@ def main():
     pix = pair.fixed.shape[0] * pair.fixed.shape[1] * pair.fixed.shape[2]
 
     def step():
-        cgs.search(cost, mov, fix, grid, costs=costs, result=res, stream=stream, points_per_warp=args.points_per_warp)
+        cgs.search(cost, mov, fix, grid, costs=costs, result=res, stream=stream, points_per_warp=args.points_per_warp,
+                   quad_taps={"auto": None, "quad": True, "texture": False}[args.taps])
 
     def barrier():
         if world > 1:
@@ -420,6 +423,7 @@ def main():
                                                           f"{S.DEFAULT_SEED}+rank)",
             "config": {"workload": WORKLOADS[args.workload] + (" (3^8 grid)" if args.small else ""), "cost": cost,
                        "grid_points": n, "pixels": pix, "points_per_warp": args.points_per_warp or "tuned",
+                       "taps": args.taps,
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_total / args.steps},

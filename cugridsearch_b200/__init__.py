@@ -28,7 +28,8 @@ from ._abi import COSTS, CgsArgmin, CgsBatchPlan, CgsError, CgsGrid, CgsImage, C
 
 __all__ = [
     "CudaGrid", "CudaImage", "CudaTensor", "CudaGridSearcher", "Argmin", "search", "argmin",
-    "COSTS", "CgsError", "library", "averageAbsoluteDifference", "averageAbsoluteDifferenceH",
+    "COSTS", "CgsError", "library", "refine", "homography", "transform_image", "fuse_aligned",
+    "filter_image", "quantize_image", "averageAbsoluteDifference", "averageAbsoluteDifferenceH",
     "sumOfAbsoluteDifferences", "sumOfAbsoluteDifferences_by_reference", "calcSQD", "calcNCC",
     "calcSQDAlt", "calcNCCAlt", "calcMIAlt", "ZNCC", "MI", "Batch", "BatchPair", "BatchPlan",
 ]
@@ -197,10 +198,15 @@ class CudaTensor:
 
 
 def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0,
-             warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool | None = None) -> CgsOptions:
+             warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool | None = None,
+             quad_taps: bool | None = None) -> CgsOptions:
     if cost not in COSTS:
         raise ValueError(f"unknown cost {cost!r}")
     flags = _abi.FLAG_NATURAL_ORDER if natural_order else 0
+    if quad_taps is True:
+        flags |= _abi.FLAG_QUAD_TAPS
+    elif quad_taps is False:
+        flags |= _abi.FLAG_TEXTURE_TAPS
     if exact_samples is True:
         flags |= _abi.FLAG_EXACT_SAMPLES
     elif exact_samples is False:
@@ -210,12 +216,15 @@ def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_
 
 def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs=None, stream=None,
            mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0, warps_per_block: int = 0,
-           natural_order: bool = False, exact_samples: bool | None = None, result=None) -> Argmin | None:
+           natural_order: bool = False, exact_samples: bool | None = None, result=None,
+           quad_taps: bool | None = None) -> Argmin | None:
     """Run one fused search.  With ``result`` (a CUDA uint8 tensor of sizeof(cgs_argmin)
     bytes) the call is asynchronous and returns None; otherwise it synchronises and
     returns the :class:`Argmin`.  ``exact_samples``: None = the cost's default (exact for
-    the reference functors, fast for ZNCC / MI), True / False force a mode."""
-    opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples)
+    the reference functors, fast for ZNCC / MI), True / False force a mode.  ``quad_taps``:
+    None = the library's choice, True = pre-gathered 16-byte quads, False = texture gathers."""
+    opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples,
+                   quad_taps)
     cptr = costs.data_ptr() if costs is not None else None
     s = _stream_handle(stream)
     L = _abi.load()
@@ -227,6 +236,62 @@ def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs
     check(L.cgs_search_sync(C.byref(moving.img), C.byref(fixed.img), C.byref(grid.g), C.byref(opt), cptr,
                             C.byref(r), s))
     return Argmin.from_struct(r)
+
+
+def refine(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, depth: int, stream=None,
+           mi_bins: int = 0, overlap_gate: float = 0.0, exact_samples: bool | None = None):
+    """Coarse-to-fine search (cgs_search_refine): `depth` searches, each on the previous grid
+    shrunk about its argmin as the reference's driver does (src/gpu/cudaGridSearch_main_mi.cu:
+    312-363).  Returns (per-level Argmins, the last level's CudaGrid)."""
+    opt = _options(cost, mi_bins, overlap_gate, exact_samples=exact_samples)
+    levels = (CgsArgmin * int(depth))()
+    last = CudaGrid(grid.g.dims)
+    check(_abi.load().cgs_search_refine(C.byref(moving.img), C.byref(fixed.img), C.byref(grid.g), C.byref(opt),
+                                        int(depth), levels, C.byref(last.g), _stream_handle(stream)))
+    return [Argmin.from_struct(r) for r in levels], last
+
+
+def homography(params, cx: float = 0.0, cy: float = 0.0, centred: bool = True) -> np.ndarray:
+    """parametersToHomography (centred at (cx, cy)) or the uncentred form: the 8 entries
+    h11..h32 (float32) of the reference's float arithmetic."""
+    p = (C.c_float * 8)(*[float(np.float32(v)) for v in params])
+    out = (C.c_float * 8)()
+    check(_abi.load().cgs_homography(p, float(cx), float(cy), int(bool(centred)), out))
+    return np.array(list(out), np.float32)
+
+
+def transform_image(H, image: CudaImage, out: CudaImage, rows: int | None = None, cols: int | None = None,
+                    stream=None) -> None:
+    """transformImage: out(y, x) = image sampled at the inverse map of H, where inside."""
+    h = (C.c_float * 8)(*[float(np.float32(v)) for v in H])
+    rows = out.height() if rows is None else rows
+    cols = out.width() if cols is None else cols
+    check(_abi.load().cgs_transform_image(h, int(rows), int(cols), C.byref(image.img), C.byref(out.img),
+                                          _stream_handle(stream)))
+
+
+def fuse_aligned(estimated_H, true_H, reference: CudaImage, moving: CudaImage, fused: CudaImage, channel: int = 0,
+                 stream=None) -> None:
+    """fuseAlignedImages: 3-channel overlay (moving under the estimate, reference, moving
+    under the true homography)."""
+    he = (C.c_float * 8)(*[float(np.float32(v)) for v in estimated_H])
+    ht = (C.c_float * 8)(*[float(np.float32(v)) for v in true_H])
+    check(_abi.load().cgs_fuse_aligned(he, ht, C.byref(reference.img), C.byref(moving.img), C.byref(fused.img),
+                                       int(channel), _stream_handle(stream)))
+
+
+def filter_image(filt: CudaImage, image: CudaImage, out: CudaImage, actions=None, stream=None) -> None:
+    """CudaImage::filter: correlate FILTER channels (action 1) with `filt`, copy COPY channels
+    (action 0); by default every channel is filtered."""
+    c = image.channels()
+    acts = (C.c_int32 * c)(*([1] * c if actions is None else [int(a) for a in actions]))
+    check(_abi.load().cgs_filter_image(C.byref(filt.img), C.byref(image.img), C.byref(out.img), acts,
+                                       _stream_handle(stream)))
+
+
+def quantize_image(image: CudaImage, mod: float, stream=None) -> None:
+    """transformPixel: in-place intensity quantisation of a uint8 image."""
+    check(_abi.load().cgs_quantize_image(C.byref(image.img), float(mod), _stream_handle(stream)))
 
 
 def argmin(values, stream=None) -> Argmin:

@@ -20,6 +20,8 @@ PIXEL_F32, PIXEL_U8, PIXEL_F64, PIXEL_U16 = 0, 1, 2, 3
 FLAG_NATURAL_ORDER = 1
 FLAG_EXACT_SAMPLES = 2
 FLAG_FAST_SAMPLES = 4
+FLAG_QUAD_TAPS = 8
+FLAG_TEXTURE_TAPS = 16
 
 STATUS = {
     0: "CGS_SUCCESS", 1: "CGS_ERROR_INVALID_VALUE", 2: "CGS_ERROR_UNSUPPORTED",
@@ -31,9 +33,13 @@ STATUS = {
 EXPORTS = [
     "cgs_grid_update", "cgs_grid_num_elements", "cgs_grid_point", "cgs_search",
     "cgs_argmin_f32", "cgs_search_sync", "cgs_status_string", "cgs_last_error", "cgs_version",
-    "cgs_mi_histogram", "cgs_search_noalloc", "cgs_covariance",
+    "cgs_mi_histogram", "cgs_search_noalloc", "cgs_covariance", "cgs_search_refine",
+    "cgs_homography", "cgs_transform_image", "cgs_fuse_aligned", "cgs_filter_image", "cgs_quantize_image",
     "cgs_batch_create", "cgs_batch_launch", "cgs_batch_set_plan", "cgs_batch_get_plan", "cgs_batch_autotune",
     "cgs_batch_pair_times", "cgs_batch_destroy", "cgs_search_batched", "cgs_autotune",
+    "cgs_net_param_count", "cgs_net_create", "cgs_net_destroy", "cgs_net_get_params", "cgs_net_set_params",
+    "cgs_net_get_grads", "cgs_net_forward", "cgs_net_backward", "cgs_net_adam_step", "cgs_grid_window",
+    "cgs_proposal_window",
 ]
 
 
@@ -112,6 +118,20 @@ def load() -> C.CDLL:
         L.cgs_mi_histogram.argtypes = [P(CgsImage), P(CgsImage), P(C.c_float), C.c_int32, C.c_void_p, C.c_void_p]
         L.cgs_covariance.restype = C.c_int
         L.cgs_covariance.argtypes = [P(CgsGrid), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.cgs_search_refine.restype = C.c_int
+        L.cgs_search_refine.argtypes = [P(CgsImage), P(CgsImage), P(CgsGrid), P(CgsOptions), C.c_int32,
+                                        P(CgsArgmin), P(CgsGrid), C.c_void_p]
+        L.cgs_homography.restype = C.c_int
+        L.cgs_homography.argtypes = [P(C.c_float), C.c_float, C.c_float, C.c_int32, P(C.c_float)]
+        L.cgs_transform_image.restype = C.c_int
+        L.cgs_transform_image.argtypes = [P(C.c_float), C.c_int32, C.c_int32, P(CgsImage), P(CgsImage), C.c_void_p]
+        L.cgs_fuse_aligned.restype = C.c_int
+        L.cgs_fuse_aligned.argtypes = [P(C.c_float), P(C.c_float), P(CgsImage), P(CgsImage), P(CgsImage), C.c_int32,
+                                       C.c_void_p]
+        L.cgs_filter_image.restype = C.c_int
+        L.cgs_filter_image.argtypes = [P(CgsImage), P(CgsImage), P(CgsImage), P(C.c_int32), C.c_void_p]
+        L.cgs_quantize_image.restype = C.c_int
+        L.cgs_quantize_image.argtypes = [P(CgsImage), C.c_float, C.c_void_p]
         L.cgs_batch_create.restype = C.c_int
         L.cgs_batch_create.argtypes = [P(CgsPair), C.c_int32, P(CgsBatchPlan), P(C.c_void_p)]
         L.cgs_batch_launch.restype = C.c_int
@@ -131,6 +151,27 @@ def load() -> C.CDLL:
         L.cgs_search_batched.argtypes = [P(CgsPair), C.c_int32, P(CgsBatchPlan), C.c_void_p]
         L.cgs_autotune.restype = C.c_int
         L.cgs_autotune.argtypes = [P(CgsPair), C.c_int32, C.c_int32, P(CgsBatchPlan)]
+        L.cgs_net_param_count.restype = C.c_int64
+        L.cgs_net_param_count.argtypes = []
+        L.cgs_net_create.restype = C.c_int
+        L.cgs_net_create.argtypes = [C.c_int32, C.c_uint64, P(C.c_void_p)]
+        L.cgs_net_destroy.restype = C.c_int
+        L.cgs_net_destroy.argtypes = [C.c_void_p]
+        for fn in ("cgs_net_get_params", "cgs_net_set_params", "cgs_net_get_grads"):
+            getattr(L, fn).restype = C.c_int
+            getattr(L, fn).argtypes = [C.c_void_p, P(C.c_float)]
+        L.cgs_net_forward.restype = C.c_int
+        L.cgs_net_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                      C.c_void_p]
+        L.cgs_net_backward.restype = C.c_int
+        L.cgs_net_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.cgs_net_adam_step.restype = C.c_int
+        L.cgs_net_adam_step.argtypes = [C.c_void_p, C.c_float, C.c_void_p]
+        L.cgs_grid_window.restype = C.c_int
+        L.cgs_grid_window.argtypes = [P(CgsGrid), P(C.c_int32), P(C.c_int32), P(CgsGrid)]
+        L.cgs_proposal_window.restype = C.c_int
+        L.cgs_proposal_window.argtypes = [P(CgsGrid), P(C.c_float), C.c_int32, C.c_int32, P(C.c_int32),
+                                          P(C.c_int32)]
         L.cgs_status_string.restype = C.c_char_p
         L.cgs_status_string.argtypes = [C.c_int]
         L.cgs_last_error.restype = C.c_char_p

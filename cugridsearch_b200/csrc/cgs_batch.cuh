@@ -120,12 +120,12 @@ __global__ void __launch_bounds__(NW * 32, batch_min_blocks(G, NW)) batch_kernel
         if (threadIdx.x == 0 && b.t_start) atomicMin(b.t_start + pair, (unsigned long long)global_ns());
         bool ok = true;
         switch (p.cost) {
-            case CGS_COST_SAD_AVG: ok = run_task<CGS_COST_SAD_AVG, C, G, NW, true, BSPLIT>(p, task, sm, it, prod); break;
-            case CGS_COST_SQD_REF: ok = run_task<CGS_COST_SQD_REF, C, G, NW, true, BSPLIT>(p, task, sm, it, prod); break;
-            case CGS_COST_NCC_REF: ok = run_task<CGS_COST_NCC_REF, C, G, NW, true, BSPLIT>(p, task, sm, it, prod); break;
-            case CGS_COST_ZNCC: ok = run_task<CGS_COST_ZNCC, C, G, NW, true, BSPLIT>(p, task, sm, it, prod); break;
+            case CGS_COST_SAD_AVG: ok = run_task<CGS_COST_SAD_AVG, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
+            case CGS_COST_SQD_REF: ok = run_task<CGS_COST_SQD_REF, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
+            case CGS_COST_NCC_REF: ok = run_task<CGS_COST_NCC_REF, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
+            case CGS_COST_ZNCC: ok = run_task<CGS_COST_ZNCC, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
             default:  // CGS_COST_MI: the host admits only batch_cost_supported() costs
-                ok = run_task<CGS_COST_MI, C, G, NW, false, BSPLIT>(p, task, sm, it, prod);
+                ok = run_task<CGS_COST_MI, C, G, NW, kTapsLoads, BSPLIT>(p, task, sm, it, prod);
                 break;
         }
         if (!ok) {

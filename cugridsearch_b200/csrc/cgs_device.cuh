@@ -13,11 +13,18 @@
 
 namespace cgs {
 
-// Explicitly rounded FP32 operations: never contracted into FMA by the compiler.
-__device__ __forceinline__ float xm(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float xa(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float xs(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float xd(float a, float b) { return __fdiv_rn(a, b); }
+// Explicitly rounded FP32 operations: never contracted into FMA by the compiler.  The host
+// versions are plain IEEE operations (the host build has no fused multiply-add).
+#ifdef __CUDA_ARCH__
+#define CGS_RN(dev, op) return dev(a, b)
+#else
+#define CGS_RN(dev, op) return a op b
+#endif
+__host__ __device__ __forceinline__ float xm(float a, float b) { CGS_RN(__fmul_rn, *); }
+__host__ __device__ __forceinline__ float xa(float a, float b) { CGS_RN(__fadd_rn, +); }
+__host__ __device__ __forceinline__ float xs(float a, float b) { CGS_RN(__fsub_rn, -); }
+__host__ __device__ __forceinline__ float xd(float a, float b) { CGS_RN(__fdiv_rn, /); }
+#undef CGS_RN
 
 // Homography h11..h32 (h33 = 1), row-major without h33.
 struct Homog {
@@ -28,7 +35,7 @@ struct Homog {
 // decomposition C*K*T*R*Sh*Sc*C, normalised by h33.  Parameters [theta, sx, sy, shear,
 // tx, ty, kx, ky]; c, s = cos(theta), sin(theta) from the host (same libm as the
 // reference's CPU path).  Parenthesisation follows C's parse of the reference lines.
-__device__ __forceinline__ Homog h_centred(const float *q, float c, float s, float cx, float cy) {
+__host__ __device__ __forceinline__ Homog h_centred(const float *q, float c, float s, float cx, float cy) {
     const float sx = q[1], sy = q[2], sh = q[3], tx = q[4], ty = q[5], kx = q[6], ky = q[7];
     const float a2 = xa(xm(cx, kx), 1.0f);
     const float a4 = xm(cx, ky);
@@ -58,7 +65,7 @@ __device__ __forceinline__ Homog h_centred(const float *q, float c, float s, flo
 }
 
 // Uncentred parametrisation of averageAbsoluteDifference (src/gpu/cudaErrorFunctions.cuh:42-57).
-__device__ __forceinline__ Homog h_uncentred(const float *q, float c, float s) {
+__host__ __device__ __forceinline__ Homog h_uncentred(const float *q, float c, float s) {
     const float sx = q[1], sy = q[2], sh = q[3], tx = q[4], ty = q[5];
     Homog h;
     h.h11 = xm(sx, c);

@@ -43,17 +43,20 @@ struct PrepParams {
     int32_t fix_alias;   // stage the fixed image like the moving one (scanline functors)
     float *row_table;    // calcMIAlt row values, or null
     int32_t rowsf;
+    float4 *quad_dst;    // moving-image tap quads (W x H per channel), or null
+    int64_t qplane;
 };
 
 // Staged layout of a moving/fixed image pair inside one scratch block.
 struct Staging {
     int32_t mpitch = 0, fpitch = 0;
     int64_t mplane = 0, fplane = 0;
-    size_t mov_off = 0, fix_off = 0, rows_off = 0, bytes = 0;
+    size_t mov_off = 0, fix_off = 0, rows_off = 0, quad_off = 0, bytes = 0;
+    int64_t qplane = 0;  // quads per channel (0: no quad planes)
 };
 
 Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align,
-                       bool fix_alias = false, bool row_table = false);
+                       bool fix_alias = false, bool row_table = false, bool quads = false);
 char *staging_origin(void *scratch, int tex_align);  // first tex_align boundary of a block
 bool exact_samples(int cost, int flags);             // sampling mode of a request
 
@@ -74,16 +77,16 @@ const void *batch_prep_kernel_fn();  // batch_prep_kernel(const PrepParams *), g
         if (e_ != cudaSuccess) return cgs::cuda_fail(e_, what); \
     } while (0)
 
-// Kernel of a pixel-loop cost for (channels, points per warp, warps per CTA), or null.
-using KernelGetter = const void *(*)(int C, int G, int NW);
-const void *kernel_sad_avg(int C, int G, int NW);
-const void *kernel_sad_avg_h(int C, int G, int NW);
-const void *kernel_sad_sum_t(int C, int G, int NW);
-const void *kernel_sad_sum_t_ref(int C, int G, int NW);
-const void *kernel_sqd_ref(int C, int G, int NW);
-const void *kernel_ncc_ref(int C, int G, int NW);
-const void *kernel_zncc(int C, int G, int NW);
-const void *kernel_mi(int C, int G, int NW);
+// Kernel of a pixel-loop cost for (channels, points per warp, warps per CTA, quad taps), or null.
+using KernelGetter = const void *(*)(int C, int G, int NW, bool quad);
+const void *kernel_sad_avg(int C, int G, int NW, bool quad);
+const void *kernel_sad_avg_h(int C, int G, int NW, bool quad);
+const void *kernel_sad_sum_t(int C, int G, int NW, bool quad);
+const void *kernel_sad_sum_t_ref(int C, int G, int NW, bool quad);
+const void *kernel_sqd_ref(int C, int G, int NW, bool quad);
+const void *kernel_ncc_ref(int C, int G, int NW, bool quad);
+const void *kernel_zncc(int C, int G, int NW, bool quad);
+const void *kernel_mi(int C, int G, int NW, bool quad);
 
 // Scanline functors (calcSQDAlt, calcNCCAlt, calcMIAlt) and their shared-memory size.
 const void *kernel_scan(int cost, int C);
@@ -101,18 +104,22 @@ const void *kernel_zncc_loads(int C);
 
 }  // namespace cgs
 
-// Instantiates search_kernel<COST, C, G, NW> for C in {1, 3}, G in {1, 2, 4}, NW in {8, 16}.
-#define CGS_KERNEL_CASES(COST, C, NWV)                                                        \
-    if (G == 1) return (const void *)search_kernel<COST, C, 1, NWV>;                          \
-    if (G == 2) return (const void *)search_kernel<COST, C, 2, NWV>;                          \
-    if (G == 4) return (const void *)search_kernel<COST, C, 4, NWV>;
+// Instantiates search_kernel<COST, C, G, NW, taps> for C in {1, 3}, G in {1, 2, 4}, NW in
+// {8, 16}, with the cost's default taps or quad taps.
+#define CGS_KERNEL_CASES(COST, C, NWV, TP)                                                    \
+    if (G == 1) return (const void *)search_kernel<COST, C, 1, NWV, TP>;                      \
+    if (G == 2) return (const void *)search_kernel<COST, C, 2, NWV, TP>;                      \
+    if (G == 4) return (const void *)search_kernel<COST, C, 4, NWV, TP>;
+#define CGS_KERNEL_SHAPES(COST, TP)                                                            \
+    if (C == 1 && NW == 16) { CGS_KERNEL_CASES(COST, 1, 16, TP) }                             \
+    if (C == 3 && NW == 16) { CGS_KERNEL_CASES(COST, 3, 16, TP) }                             \
+    if (C == 1 && NW == 8) { CGS_KERNEL_CASES(COST, 1, 8, TP) }                               \
+    if (C == 3 && NW == 8) { CGS_KERNEL_CASES(COST, 3, 8, TP) }
 #define CGS_DEFINE_KERNEL_GETTER(NAME, COST)                                                   \
     namespace cgs {                                                                           \
-    const void *NAME(int C, int G, int NW) {                                                  \
-        if (C == 1 && NW == 16) { CGS_KERNEL_CASES(COST, 1, 16) }                             \
-        if (C == 3 && NW == 16) { CGS_KERNEL_CASES(COST, 3, 16) }                             \
-        if (C == 1 && NW == 8) { CGS_KERNEL_CASES(COST, 1, 8) }                               \
-        if (C == 3 && NW == 8) { CGS_KERNEL_CASES(COST, 3, 8) }                               \
+    const void *NAME(int C, int G, int NW, bool quad) {                                       \
+        if (quad) { CGS_KERNEL_SHAPES(COST, kTapsQuad) }                                      \
+        else { CGS_KERNEL_SHAPES(COST, default_taps(COST)) }                                  \
         return nullptr;                                                                       \
     }                                                                                         \
     }
@@ -120,8 +127,8 @@ const void *kernel_zncc_loads(int C);
 #define CGS_DEFINE_LOADS_GETTER(NAME, COST)                                                    \
     namespace cgs {                                                                           \
     const void *NAME(int C) {                                                                 \
-        if (C == 1) return (const void *)search_kernel<COST, 1, 4, 16, false>;                \
-        if (C == 3) return (const void *)search_kernel<COST, 3, 4, 16, false>;                \
+        if (C == 1) return (const void *)search_kernel<COST, 1, 4, 16, kTapsLoads>;           \
+        if (C == 3) return (const void *)search_kernel<COST, 3, 4, 16, kTapsLoads>;           \
         return nullptr;                                                                       \
     }                                                                                         \
     }

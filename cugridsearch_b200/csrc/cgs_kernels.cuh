@@ -59,6 +59,9 @@ struct SearchParams {
     unsigned int *status;
     const float *vmax;   // max |moving pixel| (from the staging kernel)
     cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
+    const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y, x+1), (y+1, x), (y+1, x+1)}
+    int32_t quad_pitch;           // quads per row
+    int64_t quad_plane;           // quads per channel
     const float *row_table;       // calcMIAlt's row values (the float recurrence row += 1/(H_f-1))
     int32_t n_rows;
     cgs_argmin *result;
@@ -346,6 +349,12 @@ static __device__ void write_result(const SearchParams &p) {
 
 // ---------------------------------------------------------------- one task of a persistent CTA
 
+// How a fast-path sample reads its 2x2 taps from the staged moving image: one texture gather,
+// four cached scalar loads, or one 16-byte load of the pixel's pre-gathered quad.
+enum Taps : int { kTapsTexture = 0, kTapsLoads = 1, kTapsQuad = 2 };
+
+__host__ __device__ constexpr int default_taps(int cost) { return cost == CGS_COST_MI ? kTapsLoads : kTapsTexture; }
+
 // MI bin guard of one grid point: coordinate bounds scaled to bin units (sgx, sgy) and the
 // widest fractional tap weight that keeps the sample in its cell (hx, hy).
 struct MiGuard {
@@ -438,15 +447,13 @@ __device__ __forceinline__ void retire_tasks(const SearchParams &p, unsigned lon
 // bit-identical across those tunings.  Thread 0 calls prod.after_chunk(it) after each chunk's
 // barrier to refill the released stage.  Returns false if a bounded wait gave up (the CTA
 // stops; the task is not retired).
-template <int COST, int C, int G, int NW, bool TEX, bool BSPLIT, class Prod>
+template <int COST, int C, int G, int NW, int TAPS, bool BSPLIT, class Prod>
 __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, const CtaSmem &sm, uint32_t &it,
                                          Prod &prod) {
     constexpr int NA = AccN<COST>::value;
     constexpr bool kMI = (COST == CGS_COST_MI);
     constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
-    // taps: one texture gather per sample (fewer instructions); MI, whose extra bin-guard work
-    // leaves less latency tolerance, measured faster with four cached global loads
-    constexpr bool kTexTaps = TEX;
+    constexpr bool kTexTaps = (TAPS == kTapsTexture);
     constexpr int PSTEP = BSPLIT ? NW * 32 : 32;  // pixel stride of a lane
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -459,6 +466,9 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
     const float mrows = (float)(p.mov.h + 1);  // texture rows per plane
     const float *__restrict__ mdata = p.mov.data;
     const cudaTextureObject_t mtex = p.mov_tex;
+    const float4 *__restrict__ mquad = p.mov_quad;
+    const int qpitch = p.quad_pitch;
+    const int64_t qplane = p.quad_plane;
     const float mov_wf = p.mov_wf, mov_hf = p.mov_hf;
     const float hw = 0.5f * mov_wf, hh = 0.5f * mov_hf;
     const int B = p.mi_bins;
@@ -666,7 +676,9 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                     const float fx = tx - kMagic, fy = ty - kMagic;
                     const float ax = mxs[g] - fx, ay = mys[g] - fy;
                     const float u = fin[g] ? fx + 1.0f : -4.0f;
-                    const int base = fin[g] ? (__float_as_int(tx) - kMagicBits) + mpitch * (__float_as_int(ty) - kMagicBits) : 0;
+                    const int ix = __float_as_int(tx) - kMagicBits, iy = __float_as_int(ty) - kMagicBits;
+                    const int base = fin[g] ? ix + mpitch * iy : 0;
+                    const int qbase = fin[g] ? ix + qpitch * iy : 0;
 #pragma unroll
                     for (int c = 0; c < C; c++) {
                         float v00, v01, v10, v11;
@@ -674,6 +686,9 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                             const float4 t4 = tex2Dgather<float4>(mtex, u, fy + 1.0f + (float)c * mrows, 0);
                             // gather order: x = (i0, j1), y = (i1, j1), z = (i1, j0), w = (i0, j0)
                             v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
+                        } else if constexpr (TAPS == kTapsQuad) {
+                            const float4 q4 = __ldg(mquad + c * qplane + qbase);
+                            v00 = q4.x; v01 = q4.y; v10 = q4.z; v11 = q4.w;
                         } else {
                             const float *pl = mdata + c * mplane + base;
                             v00 = __ldg(pl); v01 = __ldg(pl + 1);
@@ -886,7 +901,7 @@ struct StaticProducer {
 
 // NW warps per CTA; 512 / (32 NW) CTAs share an SM (two CTAs of 8 warps hide each
 // other's chunk barriers).  Tasks are dealt round-robin over the persistent CTAs.
-template <int COST, int C, int G, int NW, bool TEX = (COST != CGS_COST_MI)>
+template <int COST, int C, int G, int NW, int TAPS = default_taps(COST)>
 __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_constant__ SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const CtaSmem sm = carve_smem<G, NW>(smem, p.chunk_rows * p.fix.pitch * C);
@@ -906,7 +921,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) search_kernel(const __grid_c
 
     uint32_t it = 0;
     for (uint32_t k = 0; k < my_tasks; k++) {
-        if (!run_task<COST, C, G, NW, TEX, false>(p, blockIdx.x + k * gridDim.x, sm, it, prod)) {
+        if (!run_task<COST, C, G, NW, TAPS, false>(p, blockIdx.x + k * gridDim.x, sm, it, prod)) {
             // a bounded wait gave up: retire this CTA's remaining tasks with the timeout status
             if (threadIdx.x == 0) retire_tasks(p, ~0ull, my_tasks - k, true);
             return;

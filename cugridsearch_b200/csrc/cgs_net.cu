@@ -1,0 +1,821 @@
+// cgs_net.cu -- the learned proposal network: a small CNN that looks at an image pair and
+// predicts where the grid search's argmin lies (a centre per parameter) and how sure it is
+// (a log-radius per parameter), trained and run with hand-written sm_100a kernels.
+//
+// Architecture.  Input: the pair box-averaged to 128 x 128, fixed and moving as 2 channels,
+// (v - 127.5) / 64.  Five 3x3 stride-2 convolutions (pad 1, channels 32-64-128-128-256, ReLU):
+// 128 -> 64 -> 32 -> 16 -> 8 -> 4; global average pool (256); fc 256 -> 128 + ReLU; fc
+// 128 -> 16 (8 centres in [-1, 1] grid-range units, 8 log-radii).
+//
+// Numerics.  Activations are NHWC BF16, weights FP32 masters with BF16 copies; every
+// convolution (forward, data gradient, weight gradient) is an implicit GEMM on the BF16 tensor
+// cores (mma.sync m16n8k16, FP32 accumulation); pooling, the MLP, the loss and Adam run in FP32.
+//
+// Loss.  Laplace negative log-likelihood of the label y per parameter: |c - y| e^-s + s with
+// s clamped to [-6, 4] (no gradient outside), averaged over batch and parameters.
+//
+// Parameters are one flat FP32 vector: for each conv layer W [Cout][Kp] (Kp = 9 Cin rounded up
+// to 32, the padding zero) then b [Cout]; fc1 W [128][256], b [128]; fc2 W [16][128], b [16].
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "cgs_internal.h"
+
+typedef __nv_bfloat16 bf16;
+
+namespace cgs {
+namespace net {
+
+constexpr int kLayers = 5;
+constexpr int kCin[kLayers] = {2, 32, 64, 128, 128};
+constexpr int kCout[kLayers] = {32, 64, 128, 128, 256};
+constexpr int kSide = 128;  // input side; layer l output side = 64 >> l
+constexpr int kFeat = 256, kHid = 128, kOut = 16, kParams8 = 8;
+
+__host__ __device__ constexpr int side_in(int l) { return kSide >> l; }
+__host__ __device__ constexpr int side_out(int l) { return kSide >> (l + 1); }
+constexpr int kdim(int l) { return 9 * kCin[l]; }
+constexpr int kpad(int l) { return (kdim(l) + 31) / 32 * 32; }
+
+// Offsets of the flat parameter vector.
+struct Layout {
+    int64_t w[kLayers], b[kLayers];
+    int64_t fc1w, fc1b, fc2w, fc2b, total;
+    Layout() {
+        int64_t o = 0;
+        for (int l = 0; l < kLayers; l++) {
+            w[l] = o;
+            o += (int64_t)kCout[l] * kpad(l);
+            b[l] = o;
+            o += kCout[l];
+        }
+        fc1w = o;
+        o += (int64_t)kHid * kFeat;
+        fc1b = o;
+        o += kHid;
+        fc2w = o;
+        o += (int64_t)kOut * kHid;
+        fc2b = o;
+        o += kOut;
+        total = o;
+    }
+};
+
+// ---------------------------------------------------------------- tensor-core tile
+
+constexpr int BM = 64, BN = 64, BK = 32, PAD = 8, LDS = BK + PAD;  // smem row: 80 bytes
+constexpr int kThreads = 128;                                        // 4 warps, 32 x 32 each
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// A warp's 32 x 32 block of C += A[BM x BK] B[BK x BN] for one BK slice.  As is [BM][LDS] and
+// Bs is [BN][LDS], both k-contiguous.  Fragments of m16n8k16 (g = lane / 4, t = lane % 4):
+// A regs {row g, k 2t..}, {row g+8, k 2t..}, {row g, k 2t+8..}, {row g+8, k 2t+8..};
+// B regs {k 2t.., col g}, {k 2t+8.., col g}; C {row g, col 2t, 2t+1}, {row g+8, col 2t, 2t+1}.
+__device__ __forceinline__ void warp_mma(const bf16 *As, const bf16 *Bs, int wm, int wn, float (&acc)[2][4][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+        uint32_t a[2][4], b[4][2];
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const bf16 *p = As + (wm + i * 16 + g) * LDS + kk + 2 * t;
+            a[i][0] = *reinterpret_cast<const uint32_t *>(p);
+            a[i][1] = *reinterpret_cast<const uint32_t *>(p + 8 * LDS);
+            a[i][2] = *reinterpret_cast<const uint32_t *>(p + 8);
+            a[i][3] = *reinterpret_cast<const uint32_t *>(p + 8 * LDS + 8);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bf16 *p = Bs + (wn + j * 8 + g) * LDS + kk + 2 * t;
+            b[j][0] = *reinterpret_cast<const uint32_t *>(p);
+            b[j][1] = *reinterpret_cast<const uint32_t *>(p + 8);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], a[i], b[j]);
+    }
+}
+
+// Output coordinates of accumulator element (i, j, r) of warp (wm, wn) in a tile at (m0, n0).
+__device__ __forceinline__ void acc_coord(int m0, int n0, int wm, int wn, int i, int j, int r, int &m, int &n) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    m = m0 + wm + i * 16 + g + ((r & 2) ? 8 : 0);
+    n = n0 + wn + j * 8 + 2 * t + (r & 1);
+}
+
+// ---------------------------------------------------------------- convolution problems
+
+// Geometry of conv layer l on a batch of n: input [n][H][H][Cin], output [n][Ho][Ho][Cout].
+struct ConvGeom {
+    int n, H, Ho, Cin, Cout, K, Kp;
+};
+
+// 8 consecutive k = (tap, ci) of the im2col row of output pixel (b, ho, wo), as bf16 (zeros
+// outside the image and past K).
+__device__ __forceinline__ uint4 im2col8(const bf16 *__restrict__ x, const ConvGeom &g, int b, int ho, int wo,
+                                         int k8) {
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (k8 >= g.K) return v;
+    if ((g.Cin & 7) == 0) {
+        const int tap = k8 / g.Cin, ci = k8 - tap * g.Cin;
+        const int hi = 2 * ho + tap / 3 - 1, wi = 2 * wo + tap % 3 - 1;
+        if (hi >= 0 && hi < g.H && wi >= 0 && wi < g.H)
+            v = *reinterpret_cast<const uint4 *>(x + (((int64_t)b * g.H + hi) * g.H + wi) * g.Cin + ci);
+        return v;
+    }
+    bf16 e[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int k = k8 + j;
+        e[j] = __float2bfloat16_rn(0.0f);
+        if (k < g.K) {
+            const int tap = k / g.Cin, ci = k - tap * g.Cin;
+            const int hi = 2 * ho + tap / 3 - 1, wi = 2 * wo + tap % 3 - 1;
+            if (hi >= 0 && hi < g.H && wi >= 0 && wi < g.H) e[j] = x[(((int64_t)b * g.H + hi) * g.H + wi) * g.Cin + ci];
+        }
+    }
+    memcpy(&v, e, 16);
+    return v;
+}
+
+// Forward: y[m][co] = relu(sum_k im2col(m, k) w[co][k] + bias[co]), m = (b, ho, wo).
+__global__ void __launch_bounds__(kThreads) conv_fwd_kernel(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
+                                                            const float *__restrict__ bias, bf16 *__restrict__ y,
+                                                            const ConvGeom g) {
+    __shared__ __align__(16) bf16 As[BM * LDS];
+    __shared__ __align__(16) bf16 Bs[BN * LDS];
+    const int M = g.n * g.Ho * g.Ho;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int warp = threadIdx.x >> 5, wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4] = {};
+    for (int k0 = 0; k0 < g.Kp; k0 += BK) {
+#pragma unroll
+        for (int rep = 0; rep < 2; rep++) {
+            const int c = threadIdx.x + rep * kThreads;
+            const int row = c >> 2, k8 = k0 + (c & 3) * 8;
+            const int m = m0 + row;
+            uint4 va = make_uint4(0, 0, 0, 0);
+            if (m < M) {
+                const int b = m / (g.Ho * g.Ho), r = m - b * g.Ho * g.Ho, ho = r / g.Ho, wo = r - ho * g.Ho;
+                va = im2col8(x, g, b, ho, wo, k8);
+            }
+            *reinterpret_cast<uint4 *>(As + row * LDS + (c & 3) * 8) = va;
+            const int co = n0 + row;
+            uint4 vb = make_uint4(0, 0, 0, 0);
+            if (co < g.Cout) vb = *reinterpret_cast<const uint4 *>(w + (int64_t)co * g.Kp + k8);
+            *reinterpret_cast<uint4 *>(Bs + row * LDS + (c & 3) * 8) = vb;
+        }
+        __syncthreads();
+        warp_mma(As, Bs, wm, wn, acc);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int r = 0; r < 4; r += 2) {
+                int m, co;
+                acc_coord(m0, n0, wm, wn, i, j, r, m, co);
+                if (m < M && co < g.Cout) {
+                    const float v0 = fmaxf(acc[i][j][r] + bias[co], 0.0f);
+                    const float v1 = fmaxf(acc[i][j][r + 1] + bias[co + 1], 0.0f);
+                    *reinterpret_cast<__nv_bfloat162 *>(y + (int64_t)m * g.Cout + co) = __floats2bfloat162_rn(v0, v1);
+                }
+            }
+}
+
+// Data gradient: dx[m][ci] = sum_{tap, co} dy[pixel reached by tap][co] wt[ci][tap][co], m =
+// (b, hi, wi) an input pixel; masked by the previous layer's ReLU (xprev > 0) and stored as
+// that layer's output gradient.  Cout is a multiple of 8, so 8 consecutive k share a tap.
+__global__ void __launch_bounds__(kThreads) conv_bwd_data_kernel(const bf16 *__restrict__ dy,
+                                                                 const bf16 *__restrict__ wt,
+                                                                 const bf16 *__restrict__ xprev,
+                                                                 bf16 *__restrict__ dx, const ConvGeom g) {
+    __shared__ __align__(16) bf16 As[BM * LDS];
+    __shared__ __align__(16) bf16 Bs[BN * LDS];
+    const int M = g.n * g.H * g.H;
+    const int KD = 9 * g.Cout;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int warp = threadIdx.x >> 5, wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4] = {};
+    for (int k0 = 0; k0 < KD; k0 += BK) {
+#pragma unroll
+        for (int rep = 0; rep < 2; rep++) {
+            const int c = threadIdx.x + rep * kThreads;
+            const int row = c >> 2, k8 = k0 + (c & 3) * 8;
+            const int m = m0 + row;
+            uint4 va = make_uint4(0, 0, 0, 0);
+            if (m < M) {
+                const int b = m / (g.H * g.H), r = m - b * g.H * g.H, hi = r / g.H, wi = r - hi * g.H;
+                const int tap = k8 / g.Cout, co = k8 - tap * g.Cout;
+                const int ho2 = hi + 1 - tap / 3, wo2 = wi + 1 - tap % 3;
+                if (ho2 >= 0 && wo2 >= 0 && !(ho2 & 1) && !(wo2 & 1) && (ho2 >> 1) < g.Ho && (wo2 >> 1) < g.Ho)
+                    va = *reinterpret_cast<const uint4 *>(
+                        dy + (((int64_t)b * g.Ho + (ho2 >> 1)) * g.Ho + (wo2 >> 1)) * g.Cout + co);
+            }
+            *reinterpret_cast<uint4 *>(As + row * LDS + (c & 3) * 8) = va;
+            const int ci = n0 + row;
+            uint4 vb = make_uint4(0, 0, 0, 0);
+            if (ci < g.Cin) vb = *reinterpret_cast<const uint4 *>(wt + (int64_t)ci * KD + k8);
+            *reinterpret_cast<uint4 *>(Bs + row * LDS + (c & 3) * 8) = vb;
+        }
+        __syncthreads();
+        warp_mma(As, Bs, wm, wn, acc);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int r = 0; r < 4; r += 2) {
+                int m, ci;
+                acc_coord(m0, n0, wm, wn, i, j, r, m, ci);
+                if (m < M && ci < g.Cin) {
+                    const int64_t o = (int64_t)m * g.Cin + ci;
+                    const float p0 = __bfloat162float(xprev[o]), p1 = __bfloat162float(xprev[o + 1]);
+                    *reinterpret_cast<__nv_bfloat162 *>(dx + o) =
+                        __floats2bfloat162_rn(p0 > 0.0f ? acc[i][j][r] : 0.0f, p1 > 0.0f ? acc[i][j][r + 1] : 0.0f);
+                }
+            }
+}
+
+// Weight gradient, split over pixels: part[z][co][k] = sum over pixel tiles of split z of
+// dy[p][co] im2col(p, k).  M' = Cout, N' = Kp, K' = pixels; both operands are gathered with
+// pixels innermost in shared memory.
+__global__ void __launch_bounds__(kThreads) conv_bwd_weight_kernel(const bf16 *__restrict__ dy,
+                                                                   const bf16 *__restrict__ x, float *__restrict__ part,
+                                                                   const ConvGeom g, int tiles_per_split) {
+    __shared__ __align__(16) bf16 As[BM * LDS];
+    __shared__ __align__(16) bf16 Bs[BN * LDS];
+    const int P = g.n * g.Ho * g.Ho;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int warp = threadIdx.x >> 5, wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4] = {};
+    const int t_begin = blockIdx.z * tiles_per_split;
+    const int t_end = min(t_begin + tiles_per_split, (P + BK - 1) / BK);
+    for (int tile = t_begin; tile < t_end; tile++) {
+        const int p0 = tile * BK;
+        // each thread: pixel pl = tid % 32, 8-wide channel groups (tid / 32) + 4 * rep
+#pragma unroll
+        for (int rep = 0; rep < 2; rep++) {
+            const int pl = threadIdx.x & 31, grp = (threadIdx.x >> 5) + rep * 4;  // 8 groups of 8 rows
+            const int p = p0 + pl;
+            const bool pv = p < P;
+            int b = 0, ho = 0, wo = 0;
+            if (pv) {
+                b = p / (g.Ho * g.Ho);
+                const int r = p - b * g.Ho * g.Ho;
+                ho = r / g.Ho;
+                wo = r - ho * g.Ho;
+            }
+            const int co = m0 + grp * 8;
+            uint4 va = make_uint4(0, 0, 0, 0);
+            if (pv && co < g.Cout) va = *reinterpret_cast<const uint4 *>(dy + (int64_t)p * g.Cout + co);
+            const bf16 *ea = reinterpret_cast<const bf16 *>(&va);
+#pragma unroll
+            for (int j = 0; j < 8; j++) As[(grp * 8 + j) * LDS + pl] = ea[j];
+            const int k8 = n0 + grp * 8;
+            uint4 vb = make_uint4(0, 0, 0, 0);
+            if (pv) vb = im2col8(x, g, b, ho, wo, k8);
+            const bf16 *eb = reinterpret_cast<const bf16 *>(&vb);
+#pragma unroll
+            for (int j = 0; j < 8; j++) Bs[(grp * 8 + j) * LDS + pl] = eb[j];
+        }
+        __syncthreads();
+        warp_mma(As, Bs, wm, wn, acc);
+        __syncthreads();
+    }
+    float *out = part + (int64_t)blockIdx.z * g.Cout * g.Kp;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                int co, k;
+                acc_coord(m0, n0, wm, wn, i, j, r, co, k);
+                if (co < g.Cout && k < g.Kp) out[(int64_t)co * g.Kp + k] = acc[i][j][r];
+            }
+}
+
+// dst[i] = sum_z part[z][i] in split order (deterministic).
+__global__ void sum_splits_kernel(const float *__restrict__ part, int splits, int64_t n, float *__restrict__ dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int z = 0; z < splits; z++) s += part[(int64_t)z * n + i];
+        dst[i] = s;
+    }
+}
+
+// Bias gradient partials: part[chunk][c] = sum of dy[p][c] over the chunk's pixels.
+__global__ void bias_grad_kernel(const bf16 *__restrict__ dy, int P, int C, int chunk, float *__restrict__ part) {
+    const int c = threadIdx.x;
+    if (c >= C) return;
+    const int p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
+    float s = 0.0f;
+    for (int p = p0; p < p1; p++) s += __bfloat162float(dy[(int64_t)p * C + c]);
+    part[(int64_t)blockIdx.x * C + c] = s;
+}
+
+// ---------------------------------------------------------------- input, pooling, MLP, loss
+
+// x0[b][y][x][0] = fixed, [..][1] = moving, each the s x s box average of an (s 128)^2 image,
+// normalised as (v - 127.5) / 64.
+__global__ void input_kernel(const float *__restrict__ fixed, const float *__restrict__ moving, int n, int s,
+                             bf16 *__restrict__ x0) {
+    const int64_t total = (int64_t)n * kSide * kSide;
+    const int side = kSide * s;
+    const float inv = 1.0f / (float)(s * s);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(i / (kSide * kSide));
+        const int r = (int)(i - (int64_t)b * kSide * kSide), yy = r / kSide, xx = r - yy * kSide;
+        float f = 0.0f, m = 0.0f;
+        for (int dy = 0; dy < s; dy++)
+            for (int dx = 0; dx < s; dx++) {
+                const int64_t o = ((int64_t)b * side + yy * s + dy) * side + xx * s + dx;
+                f += fixed[o];
+                m += moving[o];
+            }
+        x0[2 * i] = __float2bfloat16_rn((f * inv - 127.5f) * (1.0f / 64.0f));
+        x0[2 * i + 1] = __float2bfloat16_rn((m * inv - 127.5f) * (1.0f / 64.0f));
+    }
+}
+
+// feat[b][c] = mean of y5[b][16 positions][c].
+__global__ void gap_kernel(const bf16 *__restrict__ y5, int n, float *__restrict__ feat) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * kFeat) return;
+    const int b = i / kFeat, c = i - b * kFeat;
+    float s = 0.0f;
+    for (int p = 0; p < 16; p++) s += __bfloat162float(y5[((int64_t)b * 16 + p) * kFeat + c]);
+    feat[i] = s * (1.0f / 16.0f);
+}
+
+// out[b][j] = act(sum_i w[j][i] in[b][i] + bias[j]); act = ReLU when relu != 0.
+__global__ void fc_kernel(const float *__restrict__ in, const float *__restrict__ w, const float *__restrict__ bias,
+                          int n, int nin, int nout, int relu, float *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * nout) return;
+    const int b = i / nout, j = i - b * nout;
+    float s = bias[j];
+    for (int k = 0; k < nin; k++) s = fmaf(w[(int64_t)j * nin + k], in[(int64_t)b * nin + k], s);
+    out[i] = relu ? fmaxf(s, 0.0f) : s;
+}
+
+constexpr float kSMin = -6.0f, kSMax = 4.0f;
+
+// Laplace NLL per (sample, parameter) and its gradient w.r.t. the 16 outputs; lossp[b] = the
+// sample's share of the mean loss.
+__global__ void loss_kernel(const float *__restrict__ out, const float *__restrict__ labels, int n,
+                            float *__restrict__ dout, float *__restrict__ lossp) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const float scale = 1.0f / (float)(n * kParams8);
+    float L = 0.0f;
+    for (int a = 0; a < kParams8; a++) {
+        const float c = out[b * kOut + a], sr = out[b * kOut + 8 + a], y = labels[b * kParams8 + a];
+        const float s = fminf(fmaxf(sr, kSMin), kSMax);
+        const float e = fabsf(c - y), is = expf(-s);
+        L += (e * is + s) * scale;
+        dout[b * kOut + a] = (c > y ? is : (c < y ? -is : 0.0f)) * scale;
+        dout[b * kOut + 8 + a] = (sr > kSMin && sr < kSMax) ? (1.0f - e * is) * scale : 0.0f;
+    }
+    lossp[b] = L;
+}
+
+// Backward of a dense layer (one thread per output): din[b][i] = mask * sum_j w[j][i] dout[b][j]
+// with mask = (in > 0) when the input came through a ReLU; dw[j][i] = sum_b dout[b][j] in[b][i];
+// db[j] = sum_b dout[b][j].
+__global__ void fc_bwd_input_kernel(const float *__restrict__ dout, const float *__restrict__ w,
+                                    const float *__restrict__ in, int n, int nin, int nout, int relu_in,
+                                    float *__restrict__ din) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * nin) return;
+    const int b = i / nin, k = i - b * nin;
+    float s = 0.0f;
+    for (int j = 0; j < nout; j++) s = fmaf(w[(int64_t)j * nin + k], dout[(int64_t)b * nout + j], s);
+    din[i] = (!relu_in || in[i] > 0.0f) ? s : 0.0f;
+}
+
+__global__ void fc_bwd_weight_kernel(const float *__restrict__ dout, const float *__restrict__ in, int n, int nin,
+                                     int nout, float *__restrict__ dw, float *__restrict__ db) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nout * (nin + 1)) return;
+    const int j = i / (nin + 1), k = i - j * (nin + 1);
+    float s = 0.0f;
+    if (k < nin) {
+        for (int b = 0; b < n; b++) s = fmaf(dout[(int64_t)b * nout + j], in[(int64_t)b * nin + k], s);
+        dw[(int64_t)j * nin + k] = s;
+    } else {
+        for (int b = 0; b < n; b++) s += dout[(int64_t)b * nout + j];
+        db[j] = s;
+    }
+}
+
+// Pooling backward through layer 5's ReLU: dy5[b][p][c] = (y5 > 0) dfeat[b][c] / 16.
+__global__ void gap_bwd_kernel(const float *__restrict__ dfeat, const bf16 *__restrict__ y5, int n,
+                               bf16 *__restrict__ dy5) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * 16 * kFeat) return;
+    const int b = i / (16 * kFeat), c = i % kFeat;
+    const float v = __bfloat162float(y5[i]) > 0.0f ? dfeat[b * kFeat + c] * (1.0f / 16.0f) : 0.0f;
+    dy5[i] = __float2bfloat16_rn(v);
+}
+
+// Adam (bias-corrected) on the flat parameters; conv weights are then copied to BF16, row-major
+// [Cout][Kp] and transposed [Cin][9][Cout] (for the data gradient).
+__global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ gr, float *__restrict__ m1,
+                            float *__restrict__ m2, int64_t n, float lr, float c1, float c2) {
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = gr[i];
+        const float a = b1 * m1[i] + (1.0f - b1) * gi;
+        const float v = b2 * m2[i] + (1.0f - b2) * gi * gi;
+        m1[i] = a;
+        m2[i] = v;
+        p[i] -= lr * (a * c1) / (sqrtf(v * c2) + eps);
+    }
+}
+
+__global__ void to_bf16_kernel(const float *__restrict__ w, int cout, int kp, int cin, bf16 *__restrict__ wb,
+                               bf16 *__restrict__ wt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cout * kp) return;
+    const int co = i / kp, k = i - co * kp;
+    const bf16 v = __float2bfloat16_rn(w[i]);
+    wb[i] = v;
+    if (wt && k < 9 * cin) {
+        const int tap = k / cin, ci = k - tap * cin;
+        wt[((int64_t)ci * 9 + tap) * cout + co] = v;
+    }
+}
+
+}  // namespace net
+}  // namespace cgs
+
+using namespace cgs;
+using namespace cgs::net;
+
+// The network: parameters, Adam moments, gradients (flat FP32), BF16 weight copies and the
+// activations and gradients of one batch of up to max_batch pairs.
+struct cgs_net {
+    int dev = -1;
+    int sms = 0;
+    int max_batch = 0;
+    int n = 0;     // batch size of the last forward
+    int64_t step = 0;
+    Layout L;
+    char *mem = nullptr;
+    float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
+    bf16 *wb[kLayers] = {}, *wt[kLayers] = {};
+    bf16 *act[kLayers + 1] = {};  // act[0] = input, act[l + 1] = conv layer l output
+    bf16 *dya = nullptr, *dyb = nullptr;  // ping-pong output gradients
+    float *feat = nullptr, *hid = nullptr, *out = nullptr, *dout = nullptr, *dhid = nullptr, *dfeat = nullptr;
+    float *lossp = nullptr;
+    float *ws = nullptr;
+    size_t ws_floats = 0;
+};
+
+namespace cgs {
+namespace net {
+
+static cgs_status sync_bf16(cgs_net *nt, cudaStream_t s) {
+    for (int l = 0; l < kLayers; l++) {
+        const int cnt = kCout[l] * kpad(l);
+        to_bf16_kernel<<<(cnt + 255) / 256, 256, 0, s>>>(nt->params + nt->L.w[l], kCout[l], kpad(l), kCin[l], nt->wb[l],
+                                                         l > 0 ? nt->wt[l] : nullptr);
+    }
+    CGS_CUDA(cudaGetLastError(), "to_bf16_kernel");
+    return CGS_SUCCESS;
+}
+
+static ConvGeom geom(int l, int n) {
+    ConvGeom g;
+    g.n = n;
+    g.H = side_in(l);
+    g.Ho = side_out(l);
+    g.Cin = kCin[l];
+    g.Cout = kCout[l];
+    g.K = kdim(l);
+    g.Kp = kpad(l);
+    return g;
+}
+
+// Splits of the weight-gradient GEMM: enough blocks to fill the GPU twice, at least 4 pixel
+// tiles each.
+static int wgrad_splits(const ConvGeom &g, int sms, int *tiles_per_split) {
+    const int tiles = (g.n * g.Ho * g.Ho + BK - 1) / BK;
+    const int base = ((g.Cout + BM - 1) / BM) * ((g.Kp + BN - 1) / BN);
+    int splits = std::max(1, std::min(tiles / 4, (2 * sms + base - 1) / base));
+    *tiles_per_split = (tiles + splits - 1) / splits;
+    splits = (tiles + *tiles_per_split - 1) / *tiles_per_split;
+    return splits;
+}
+
+static size_t ws_need(int n, int sms) {
+    size_t need = 0;
+    for (int l = 0; l < kLayers; l++) {
+        const ConvGeom g = geom(l, n);
+        int tps;
+        const int sp = wgrad_splits(g, sms, &tps);
+        need = std::max(need, (size_t)sp * g.Cout * g.Kp);
+        const int P = n * g.Ho * g.Ho, chunk = 1024;
+        need = std::max(need, (size_t)((P + chunk - 1) / chunk) * g.Cout);
+    }
+    return need;
+}
+
+}  // namespace net
+}  // namespace cgs
+
+extern "C" {
+
+int64_t cgs_net_param_count(void) { return Layout().total; }
+
+cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
+    if (!out) return fail(CGS_ERROR_INVALID_VALUE, "out is null");
+    *out = nullptr;
+    if (max_batch < 1 || max_batch > 4096) return fail(CGS_ERROR_INVALID_VALUE, "max_batch must be 1..4096");
+    cgs_status s;
+    DeviceInfo di;
+    if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+    cgs_net *nt = new cgs_net();
+    nt->dev = di.dev;
+    nt->sms = di.sms;
+    nt->max_batch = max_batch;
+    const int64_t P = nt->L.total;
+    const int64_t B = max_batch;
+    // sizes in bytes, each block 256-aligned
+    std::vector<size_t> sz;
+    sz.push_back(4 * P * 4);  // params, grads, m1, m2
+    size_t wbytes = 0;
+    for (int l = 0; l < kLayers; l++) wbytes += 2 * ((size_t)kCout[l] * kpad(l) * 2 + 256);
+    sz.push_back(wbytes);
+    size_t abytes = (size_t)B * kSide * kSide * 2 * 2 + 256;
+    size_t dmax = 0;
+    for (int l = 0; l < kLayers; l++) {
+        const size_t e = (size_t)B * side_out(l) * side_out(l) * kCout[l];
+        abytes += e * 2 + 256;
+        dmax = std::max(dmax, e);
+    }
+    sz.push_back(abytes);
+    sz.push_back(2 * (dmax * 2 + 256));
+    sz.push_back(((size_t)B * (2 * kFeat + 2 * kHid + 2 * kOut + 1)) * 4 + 7 * 256);
+    nt->ws_floats = ws_need(max_batch, di.sms);
+    sz.push_back(nt->ws_floats * 4 + 256);
+    size_t total = 0;
+    for (size_t v : sz) total += (v + 255) / 256 * 256;
+    cudaError_t e = cudaMalloc(&nt->mem, total);
+    if (e != cudaSuccess) {
+        delete nt;
+        return cuda_fail(e, "cudaMalloc (network)");
+    }
+    char *p = nt->mem;
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) / 256 * 256;
+        return r;
+    };
+    nt->params = reinterpret_cast<float *>(take(P * 4));
+    nt->grads = reinterpret_cast<float *>(take(P * 4));
+    nt->m1 = reinterpret_cast<float *>(take(P * 4));
+    nt->m2 = reinterpret_cast<float *>(take(P * 4));
+    for (int l = 0; l < kLayers; l++) {
+        nt->wb[l] = reinterpret_cast<bf16 *>(take((size_t)kCout[l] * kpad(l) * 2));
+        nt->wt[l] = reinterpret_cast<bf16 *>(take((size_t)kCout[l] * kpad(l) * 2));
+    }
+    nt->act[0] = reinterpret_cast<bf16 *>(take((size_t)B * kSide * kSide * 2 * 2));
+    for (int l = 0; l < kLayers; l++)
+        nt->act[l + 1] = reinterpret_cast<bf16 *>(take((size_t)B * side_out(l) * side_out(l) * kCout[l] * 2));
+    nt->dya = reinterpret_cast<bf16 *>(take(dmax * 2));
+    nt->dyb = reinterpret_cast<bf16 *>(take(dmax * 2));
+    nt->feat = reinterpret_cast<float *>(take((size_t)B * kFeat * 4));
+    nt->dfeat = reinterpret_cast<float *>(take((size_t)B * kFeat * 4));
+    nt->hid = reinterpret_cast<float *>(take((size_t)B * kHid * 4));
+    nt->dhid = reinterpret_cast<float *>(take((size_t)B * kHid * 4));
+    nt->out = reinterpret_cast<float *>(take((size_t)B * kOut * 4));
+    nt->dout = reinterpret_cast<float *>(take((size_t)B * kOut * 4));
+    nt->lossp = reinterpret_cast<float *>(take((size_t)B * 4));
+    nt->ws = reinterpret_cast<float *>(take(nt->ws_floats * 4));
+
+    // He-normal initialisation (std sqrt(2 / fan_in)); the last layer small so the first
+    // proposals sit at the grid centre with radius ~1 (half the range)
+    std::vector<float> h((size_t)P, 0.0f);
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<float> nd(0.0f, 1.0f);
+    for (int l = 0; l < kLayers; l++) {
+        const float sd = std::sqrt(2.0f / (float)kdim(l));
+        for (int co = 0; co < kCout[l]; co++)
+            for (int k = 0; k < kdim(l); k++) h[nt->L.w[l] + (int64_t)co * kpad(l) + k] = sd * nd(rng);
+    }
+    for (int64_t i = 0; i < (int64_t)kHid * kFeat; i++) h[nt->L.fc1w + i] = std::sqrt(2.0f / kFeat) * nd(rng);
+    for (int64_t i = 0; i < (int64_t)kOut * kHid; i++) h[nt->L.fc2w + i] = 0.01f * nd(rng);
+    e = cudaMemcpy(nt->params, h.data(), P * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(nt->m1, 0, P * 4);
+    if (e == cudaSuccess) e = cudaMemset(nt->m2, 0, P * 4);
+    if (e == cudaSuccess) e = cudaMemset(nt->grads, 0, P * 4);
+    for (int l = 1; l < kLayers && e == cudaSuccess; l++) e = cudaMemset(nt->wt[l], 0, (size_t)kCout[l] * kpad(l) * 2);
+    if (e != cudaSuccess) {
+        cudaFree(nt->mem);
+        delete nt;
+        return cuda_fail(e, "network init");
+    }
+    if ((s = sync_bf16(nt, 0)) != CGS_SUCCESS || (e = cudaDeviceSynchronize()) != cudaSuccess) {
+        cudaFree(nt->mem);
+        delete nt;
+        return s != CGS_SUCCESS ? s : cuda_fail(e, "network init");
+    }
+    *out = nt;
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_destroy(cgs_net *nt) {
+    if (!nt) return CGS_SUCCESS;
+    cudaDeviceSynchronize();
+    cudaFree(nt->mem);
+    delete nt;
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_get_params(const cgs_net *nt, float *host) {
+    if (!nt || !host) return fail(CGS_ERROR_INVALID_VALUE, "network or buffer is null");
+    CGS_CUDA(cudaMemcpy(host, nt->params, nt->L.total * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_set_params(cgs_net *nt, const float *host) {
+    if (!nt || !host) return fail(CGS_ERROR_INVALID_VALUE, "network or buffer is null");
+    CGS_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    CGS_CUDA(cudaMemcpy(nt->params, host, nt->L.total * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+    cgs_status s = sync_bf16(nt, 0);
+    if (s != CGS_SUCCESS) return s;
+    CGS_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_get_grads(const cgs_net *nt, float *host) {
+    if (!nt || !host) return fail(CGS_ERROR_INVALID_VALUE, "network or buffer is null");
+    CGS_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    CGS_CUDA(cudaMemcpy(host, nt->grads, nt->L.total * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_forward(cgs_net *nt, const float *fixed, const float *moving, int32_t n, int32_t side, float *out,
+                           cgs_stream_t stream_) {
+    if (!nt || !fixed || !moving) return fail(CGS_ERROR_INVALID_VALUE, "network or images are null");
+    if (n < 1 || n > nt->max_batch) return fail(CGS_ERROR_INVALID_VALUE, "batch size out of range");
+    if (side < kSide || side % kSide) return fail(CGS_ERROR_INVALID_VALUE, "image side must be a multiple of 128");
+    cudaStream_t s = (cudaStream_t)stream_;
+    nt->n = n;
+    const int64_t tot = (int64_t)n * kSide * kSide;
+    input_kernel<<<(int)std::min<int64_t>((tot + 255) / 256, nt->sms * 16), 256, 0, s>>>(fixed, moving, n,
+                                                                                          side / kSide, nt->act[0]);
+    for (int l = 0; l < kLayers; l++) {
+        const ConvGeom g = geom(l, n);
+        const int M = n * g.Ho * g.Ho;
+        conv_fwd_kernel<<<dim3((M + BM - 1) / BM, (g.Cout + BN - 1) / BN), kThreads, 0, s>>>(
+            nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nt->act[l + 1], g);
+    }
+    gap_kernel<<<(n * kFeat + 255) / 256, 256, 0, s>>>(nt->act[kLayers], n, nt->feat);
+    fc_kernel<<<(n * kHid + 255) / 256, 256, 0, s>>>(nt->feat, nt->params + nt->L.fc1w, nt->params + nt->L.fc1b, n,
+                                                     kFeat, kHid, 1, nt->hid);
+    fc_kernel<<<(n * kOut + 255) / 256, 256, 0, s>>>(nt->hid, nt->params + nt->L.fc2w, nt->params + nt->L.fc2b, n,
+                                                     kHid, kOut, 0, nt->out);
+    CGS_CUDA(cudaGetLastError(), "network forward");
+    if (out) CGS_CUDA(cudaMemcpyAsync(out, nt->out, (size_t)n * kOut * 4, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_backward(cgs_net *nt, const float *labels, float *loss, cgs_stream_t stream_) {
+    if (!nt || !labels) return fail(CGS_ERROR_INVALID_VALUE, "network or labels are null");
+    if (nt->n < 1) return fail(CGS_ERROR_INVALID_VALUE, "no forward pass to differentiate");
+    cudaStream_t s = (cudaStream_t)stream_;
+    const int n = nt->n;
+    float *G = nt->grads;
+    loss_kernel<<<(n + 127) / 128, 128, 0, s>>>(nt->out, labels, n, nt->dout, nt->lossp);
+    // fc2, fc1
+    fc_bwd_weight_kernel<<<(kOut * (kHid + 1) + 255) / 256, 256, 0, s>>>(nt->dout, nt->hid, n, kHid, kOut,
+                                                                         G + nt->L.fc2w, G + nt->L.fc2b);
+    fc_bwd_input_kernel<<<(n * kHid + 255) / 256, 256, 0, s>>>(nt->dout, nt->params + nt->L.fc2w, nt->hid, n, kHid,
+                                                               kOut, 1, nt->dhid);
+    fc_bwd_weight_kernel<<<(kHid * (kFeat + 1) + 255) / 256, 256, 0, s>>>(nt->dhid, nt->feat, n, kFeat, kHid,
+                                                                          G + nt->L.fc1w, G + nt->L.fc1b);
+    fc_bwd_input_kernel<<<(n * kFeat + 255) / 256, 256, 0, s>>>(nt->dhid, nt->params + nt->L.fc1w, nt->feat, n,
+                                                                kFeat, kHid, 0, nt->dfeat);
+    gap_bwd_kernel<<<(n * 16 * kFeat + 255) / 256, 256, 0, s>>>(nt->dfeat, nt->act[kLayers], n, nt->dya);
+    bf16 *dy = nt->dya, *dx = nt->dyb;
+    for (int l = kLayers - 1; l >= 0; l--) {
+        const ConvGeom g = geom(l, n);
+        int tps;
+        const int splits = wgrad_splits(g, nt->sms, &tps);
+        conv_bwd_weight_kernel<<<dim3((g.Cout + BM - 1) / BM, (g.Kp + BN - 1) / BN, splits), kThreads, 0, s>>>(
+            dy, nt->act[l], nt->ws, g, tps);
+        const int64_t wn = (int64_t)g.Cout * g.Kp;
+        sum_splits_kernel<<<(int)std::min<int64_t>((wn + 255) / 256, 1024), 256, 0, s>>>(nt->ws, splits, wn,
+                                                                                          G + nt->L.w[l]);
+        const int P = n * g.Ho * g.Ho, chunk = 1024, chunks = (P + chunk - 1) / chunk;
+        bias_grad_kernel<<<chunks, 256, 0, s>>>(dy, P, g.Cout, chunk, nt->ws);
+        sum_splits_kernel<<<1, 256, 0, s>>>(nt->ws, chunks, g.Cout, G + nt->L.b[l]);
+        if (l > 0) {
+            const int Min = n * g.H * g.H;
+            conv_bwd_data_kernel<<<dim3((Min + BM - 1) / BM, (g.Cin + BN - 1) / BN), kThreads, 0, s>>>(
+                dy, nt->wt[l], nt->act[l], dx, g);
+            std::swap(dy, dx);
+        }
+    }
+    CGS_CUDA(cudaGetLastError(), "network backward");
+    if (loss) {
+        sum_splits_kernel<<<1, 32, 0, s>>>(nt->lossp, n, 1, nt->ws);
+        CGS_CUDA(cudaMemcpyAsync(loss, nt->ws, 4, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
+    }
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_net_adam_step(cgs_net *nt, float lr, cgs_stream_t stream_) {
+    if (!nt) return fail(CGS_ERROR_INVALID_VALUE, "network is null");
+    cudaStream_t s = (cudaStream_t)stream_;
+    nt->step++;
+    const float c1 = 1.0f / (1.0f - std::pow(0.9f, (float)nt->step));
+    const float c2 = 1.0f / (1.0f - std::pow(0.999f, (float)nt->step));
+    adam_kernel<<<nt->sms * 8, 256, 0, s>>>(nt->params, nt->grads, nt->m1, nt->m2, nt->L.total, lr, c1, c2);
+    CGS_CUDA(cudaGetLastError(), "adam_kernel");
+    return sync_bf16(nt, s);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+cgs_status cgs_grid_window(const cgs_grid *full, const int32_t first[8], const int32_t count[8], cgs_grid *window) {
+    cgs_status s = check_grid(full);
+    if (s != CGS_SUCCESS) return s;
+    if (!first || !count || !window) return fail(CGS_ERROR_INVALID_VALUE, "first, count or window is null");
+    cgs_grid g = *full;
+    for (int a = 0; a < full->dims; a++) {
+        const float cnt = full->count[a];
+        if (cnt != std::floor(cnt)) return fail(CGS_ERROR_INVALID_VALUE, "grid windows need integral counts");
+        if (count[a] < 1 || first[a] < 0 || first[a] + count[a] > (int32_t)cnt)
+            return fail(CGS_ERROR_INVALID_VALUE, "window outside the grid on axis " + std::to_string(a));
+        // the full grid's own decode of the first and last index (CudaGrid::indexToGridPoint)
+        g.start[a] = std::fmaf((float)first[a], full->resolution[a], full->start[a]);
+        g.end[a] = std::fmaf((float)(first[a] + count[a] - 1), full->resolution[a], full->start[a]);
+        g.count[a] = (float)count[a];
+    }
+    if ((s = cgs_grid_update(&g, -1)) != CGS_SUCCESS) return s;
+    *window = g;
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_proposal_window(const cgs_grid *full, const float out[16], int32_t min_values, int32_t max_values,
+                               int32_t first[8], int32_t count[8]) {
+    cgs_status s = check_grid(full);
+    if (s != CGS_SUCCESS) return s;
+    if (!out || !first || !count) return fail(CGS_ERROR_INVALID_VALUE, "out, first or count is null");
+    if (min_values < 1 || max_values > 63 || min_values > max_values || !(min_values & 1) || !(max_values & 1))
+        return fail(CGS_ERROR_INVALID_VALUE, "min_values <= max_values, both odd, at most 63");
+    for (int a = 0; a < 8; a++) {
+        first[a] = 0;
+        count[a] = 1;
+    }
+    for (int a = 0; a < full->dims; a++) {
+        const float cnt = full->count[a];
+        if (cnt != std::floor(cnt)) return fail(CGS_ERROR_INVALID_VALUE, "proposal windows need integral counts");
+        const int nv = (int)cnt;
+        count[a] = nv;
+        if (nv <= 1) continue;
+        const double res = full->resolution[a], range = res * (nv - 1);
+        if (!(res > 0.0)) return fail(CGS_ERROR_INVALID_VALUE, "proposal windows need increasing axes");
+        const double c = std::isfinite(out[a]) ? std::min(1.0, std::max(-1.0, (double)out[a])) : 0.0;
+        const double sr = std::isfinite(out[8 + a]) ? std::min(4.0, std::max(-6.0, (double)out[8 + a])) : 4.0;
+        const int ic = (int)std::lround((c + 1.0) * 0.5 * (nv - 1));
+        const double radius = std::exp(sr) * 0.5 * range;
+        // every grid value within the radius of the centre: |i - ic| <= radius / res + 1/2
+        int w = (int)std::floor(radius / res + 0.5);
+        w = std::max((min_values - 1) / 2, std::min((max_values - 1) / 2, w));
+        int i0 = ic - w, i1 = ic + w;
+        if (i0 < 0) { i1 -= i0; i0 = 0; }
+        if (i1 > nv - 1) { i0 -= i1 - (nv - 1); i1 = nv - 1; }
+        i0 = std::max(i0, 0);
+        first[a] = i0;
+        count[a] = i1 - i0 + 1;
+    }
+    return CGS_SUCCESS;
+}
+
+}  // extern "C"

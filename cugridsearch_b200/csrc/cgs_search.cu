@@ -225,6 +225,22 @@ __device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int6
             v = load_pix(q.fix_src, q.fix_pix, ((y + 1) * q.fw) * q.c + c);
         q.fix_dst[i] = v;
     }
+    if (q.quad_dst) {
+        // tap quads of the staged moving plane: {P(y, x), P(y, x + 1), P(y + 1, x), P(y + 1, x + 1)}
+        // with P the padded plane (column W = the next row's pixel 0, row H = 0)
+        const int64_t qtot = q.qplane * q.c;
+        auto P = [&](int c, int64_t y, int64_t x) -> float {
+            if (y >= q.mh) return 0.0f;
+            if (x < q.mw) return load_pix(q.mov_src, q.mov_pix, (y * q.mw + x) * q.c + c);
+            return (y + 1 < q.mh) ? load_pix(q.mov_src, q.mov_pix, ((y + 1) * q.mw) * q.c + c) : 0.0f;
+        };
+        for (int64_t i = tid; i < qtot; i += nthr) {
+            const int c = (int)(i / q.qplane);
+            const int64_t e = i - (int64_t)c * q.qplane;
+            const int64_t y = e / q.mw, x = e - y * q.mw;
+            q.quad_dst[i] = make_float4(P(c, y, x), P(c, y, x + 1), P(c, y + 1, x), P(c, y + 1, x + 1));
+        }
+    }
     if (q.row_table && tid == 0) {
         // calcMIAlt's rows: row = -0.5; while (row < 0.5) row += 1 / (float)(rowsf - 1)
         // (cudaErrorFunction_mi.cuh:164), the same float additions as the reference
@@ -364,7 +380,7 @@ static int32_t mi_alt_rows(int rowsf) {
 }
 
 Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align, int tex_pitch_align,
-                              bool fix_alias, bool row_table) {
+                              bool fix_alias, bool row_table, bool quads) {
     Staging st;
     const int C = fix.channels;
     st.mpitch = (int32_t)round_up(mov.width + 1, std::max(1, tex_pitch_align / 4));
@@ -375,7 +391,9 @@ Staging staging_layout(const cgs_image &mov, const cgs_image &fix, int tex_align
     st.mov_off = (size_t)round_up(256, tex_align);
     st.fix_off = st.mov_off + (size_t)round_up(st.mplane * C * 4, 256);
     st.rows_off = st.fix_off + (size_t)round_up(st.fplane * C * 4, 256);
-    st.bytes = st.rows_off + (row_table ? (size_t)round_up((int64_t)(fix.height + 2) * 4, 256) : 0) + (size_t)tex_align;
+    st.quad_off = st.rows_off + (row_table ? (size_t)round_up((int64_t)(fix.height + 2) * 4, 256) : 0);
+    st.qplane = quads ? (int64_t)mov.width * mov.height : 0;
+    st.bytes = st.quad_off + (size_t)round_up(st.qplane * C * 16, 256) + (size_t)tex_align;
     return st;
 }
 
@@ -829,7 +847,11 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     if (!getter) return fail(CGS_ERROR_UNSUPPORTED, "cost not implemented by this build");
     const int C = fix->channels;
     const Plan pl = choose_plan(cost, o, mi_bins);
-    const void *kfn = getter(C, pl.G, pl.NW);
+    // taps: pre-gathered quads where the fast sampling path runs (measured faster than texture
+    // gathers there); texture gathers (MI: scalar loads) for exact sampling and for MI
+    const bool fast_path = !exact_samples(cost, o.flags) && cost != CGS_COST_MI;
+    const bool quads = (o.flags & CGS_FLAG_QUAD_TAPS) || (fast_path && !(o.flags & CGS_FLAG_TEXTURE_TAPS));
+    const void *kfn = getter(C, pl.G, pl.NW, quads);
     if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no kernel for this channel count / tuning");
 
     DeviceInfo di;
@@ -845,7 +867,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     }
 
     // staged layout
-    const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align);
+    const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align, false, false, quads);
     const int64_t stage_bytes = set_chunks(&p, st, C, fix->height);
     const size_t smem = cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes, acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
@@ -865,8 +887,17 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
     p.costs = costs;
     p.result = result;
+    if (quads) {
+        p.mov_quad = reinterpret_cast<const float4 *>(sb + st.quad_off);
+        p.quad_pitch = mov->width;
+        p.quad_plane = st.qplane;
+    }
 
     PrepParams q = make_prep(mov, fix, st, sb, mstage, fstage);
+    if (quads) {
+        q.quad_dst = reinterpret_cast<float4 *>(sb + st.quad_off);
+        q.qplane = st.qplane;
+    }
     const int64_t prep_elems = (st.mplane + st.fplane) * C;
     const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
     cudaError_t e = cudaMemsetAsync(sb, 0, 256, stream);
@@ -1006,7 +1037,7 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
         od.points_per_warp = 0;
         od.warps_per_block = 0;
         pl = choose_plan(cost, od, mi_bins);
-        kfn = kernel_mi(C, pl.G, pl.NW);
+        kfn = kernel_mi(C, pl.G, pl.NW, false);
     } else {
         pl.G = 4;
         pl.NW = 16;

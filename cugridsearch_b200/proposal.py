@@ -1,0 +1,468 @@
+"""The learned proposal: a CNN (``cgs_net_*`` in libcgs_b200.so) that predicts where a pair's
+grid-search argmin lies, the local grid it implies (``cgs_proposal_grid``), and the serving
+path that searches that grid and falls back to the full grid when the proposal's best cost
+is worse than a coarse probe of the full grid.
+
+The reference has no learned component; its drivers search the full grid, optionally
+shrinking the range around the argmin level by level (src/gpu/cudaGridSearch_main_mi.cu:
+312-363).  Here the full grid stays the judge: labels are the full grid's own argmins, and a
+pair whose proposal cannot beat the coarse probe is searched in full.
+
+Parameters are exchanged in grid-range units: ``u = 2 (p - start) / (end - start) - 1`` per
+axis (-1 at the grid's start, +1 at its end).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+
+N_OUT = 16
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream(stream) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream) if hasattr(s, "cuda_stream") else int(s)
+
+
+def to_units(params, start, end) -> np.ndarray:
+    """Parameters -> grid-range units (-1 .. 1 over [start, end]); collapsed axes give 0."""
+    p, a, b = (np.asarray(v, np.float64) for v in (params, start, end))
+    span = np.where(b != a, b - a, 1.0)
+    return np.where(b != a, 2.0 * (p - a) / span - 1.0, 0.0)
+
+
+def from_units(u, start, end) -> np.ndarray:
+    u, a, b = (np.asarray(v, np.float64) for v in (u, start, end))
+    return a + (u + 1.0) * 0.5 * (b - a)
+
+
+class ProposalNet:
+    """The proposal CNN on the current CUDA device (one ``cgs_net`` handle)."""
+
+    def __init__(self, max_batch: int = 256, seed: int = 0):
+        L = _abi.load()
+        h = C.c_void_p(None)
+        check(L.cgs_net_create(int(max_batch), int(seed), C.byref(h)))
+        self._h = h
+        self.max_batch = int(max_batch)
+        self.n_params = int(L.cgs_net_param_count())
+
+    # -- parameters
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        check(_abi.load().cgs_net_get_params(self._h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        if p.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {p.size}")
+        check(_abi.load().cgs_net_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def grads(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        check(_abi.load().cgs_net_get_grads(self._h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def save(self, path: str) -> None:
+        np.savez_compressed(path, params=self.params())
+
+    def load(self, path: str) -> None:
+        self.set_params(np.load(path)["params"])
+
+    # -- passes
+    def forward(self, fixed, moving, stream=None):
+        """fixed, moving: CUDA float32 tensors (n, side, side), side a multiple of 128.
+        Returns a (n, 16) CUDA tensor: 8 centres then 8 log-radii (grid-range units)."""
+        torch = _torch()
+        n, side = int(fixed.shape[0]), int(fixed.shape[-1])
+        out = torch.empty((n, N_OUT), dtype=torch.float32, device=fixed.device)
+        check(_abi.load().cgs_net_forward(self._h, fixed.data_ptr(), moving.data_ptr(), n, side, out.data_ptr(),
+                                          _stream(stream)))
+        return out
+
+    def backward(self, labels, stream=None):
+        """Gradients of the mean loss for the last forward; labels (n, 8) CUDA float32.
+        Returns the loss as a 1-element CUDA tensor."""
+        torch = _torch()
+        loss = torch.empty(1, dtype=torch.float32, device=labels.device)
+        check(_abi.load().cgs_net_backward(self._h, labels.data_ptr(), loss.data_ptr(), _stream(stream)))
+        return loss
+
+    def adam_step(self, lr: float, stream=None) -> None:
+        check(_abi.load().cgs_net_adam_step(self._h, float(lr), _stream(stream)))
+
+    def train_step(self, fixed, moving, labels, lr: float, stream=None):
+        self.forward(fixed, moving, stream)
+        loss = self.backward(labels, stream)
+        self.adam_step(lr, stream)
+        return loss
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _abi.load().cgs_net_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grid_window(full, first, count):
+    """The window of `full` with count[a] values from index first[a] on each axis (a CudaGrid
+    whose values are the full grid's)."""
+    from . import CudaGrid
+    f = (C.c_int32 * 8)(*[int(v) for v in first] + [0] * (8 - len(first)))
+    c = (C.c_int32 * 8)(*[int(v) for v in count] + [1] * (8 - len(count)))
+    g = CudaGrid(full.g.dims)
+    check(_abi.load().cgs_grid_window(C.byref(full.g), f, c, C.byref(g.g)))
+    return g
+
+
+def proposal_window(full, out16, min_values: int = 3, max_values: int = 5):
+    """(first, count) per axis of the window a proposal implies (cgs_proposal_window)."""
+    o = (C.c_float * 16)(*[float(v) for v in np.asarray(out16, np.float32)])
+    f, c = (C.c_int32 * 8)(), (C.c_int32 * 8)()
+    check(_abi.load().cgs_proposal_window(C.byref(full.g), o, int(min_values), int(max_values), f, c))
+    d = full.g.dims
+    return np.array(list(f)[:d], np.int64), np.array(list(c)[:d], np.int64)
+
+
+def proposal_grid(full, out16, min_values: int = 3, max_values: int = 5):
+    """The local grid (a CudaGrid) of one proposal."""
+    return grid_window(full, *proposal_window(full, out16, min_values, max_values))
+
+
+def coarse_grid(full, values: int = 3):
+    """A coarse probe of the full grid: on each axis `values` full-grid values a whole number of
+    steps apart (indices 0, s, 2s, .. with s = (count - 1) // (values - 1)).  Its points are
+    full-grid points, so its best cost bounds the full grid's best from above."""
+    from . import CudaGrid
+    d = full.g.dims
+    counts = [int(full.g.count[a]) for a in range(d)]
+    inc = np.cumprod([1] + counts[:-1])
+    g = CudaGrid(d)
+    for a in range(d):
+        n = counts[a]
+        k = max(1, min(values, n))
+        step = (n - 1) // (k - 1) if k > 1 else 0
+        g.g.start[a] = full.g.start[a]
+        g.g.end[a] = float(full.getGridPoint(int((k - 1) * step * inc[a]))[a]) if k > 1 else full.g.start[a]
+        g.g.count[a] = float(k)
+    g.update()
+    return g
+
+
+@dataclass
+class ServeResult:
+    params: np.ndarray   # (n, 8) chosen grid points
+    costs: np.ndarray    # (n,) their costs
+    fallback: np.ndarray # (n,) True where the full grid was searched
+    points: int          # grid points evaluated in total (proposal + probe + fallbacks)
+
+
+def full_grid(side: int = 256, values: int = 6):
+    """The full grid of the learned-proposal configuration at `side` pixels."""
+    from . import CudaGrid
+    from .synthetic import config4_ranges
+    lo, hi = config4_ranges(side)
+    return CudaGrid.from_ranges([float(v) for v in lo], [float(v) for v in hi], [values] * 8)
+
+
+def _batch_search(cost, fixed, moving, grids, device):
+    """One persistent launch over pairs i with grid grids[i]: (params (n, 8), costs (n,),
+    valid (n,), points evaluated)."""
+    import torch
+    from . import Batch, BatchPair, CudaImage, read_result, result_buffer
+    res = [result_buffer(device) for _ in grids]
+    pairs = [BatchPair(cost, CudaImage(moving[i]), CudaImage(fixed[i]), g, res[i]) for i, g in enumerate(grids)]
+    with Batch(pairs) as b:
+        b.launch()
+        torch.cuda.synchronize(device)
+    out = [read_result(r) for r in res]
+    params = np.stack([o.params for o in out]).astype(np.float64)
+    costs = np.array([o.cost for o in out], np.float64)
+    valid = np.array([o.valid and o.status == 0 for o in out])
+    return params, costs, valid, int(sum(g.numElements() for g in grids))
+
+
+def grid_argmins(fixed, moving, grid, cost: str = "ZNCC", chunk: int = 256):
+    """The grid-search argmin of every pair (the full grid's answer), in chunks of pairs per
+    persistent launch.  fixed, moving: CUDA float32 (n, side, side).  Returns (params, costs)."""
+    n = int(fixed.shape[0])
+    ps, cs = [], []
+    for i in range(0, n, chunk):
+        j = min(n, i + chunk)
+        p, c, _, _ = _batch_search(cost, fixed[i:j], moving[i:j], [grid] * (j - i), fixed.device)
+        ps.append(p)
+        cs.append(c)
+    return np.concatenate(ps), np.concatenate(cs)
+
+
+def _axis_indices(index: int, counts) -> np.ndarray:
+    """Per-axis indices of a flat grid index (axis 0 fastest)."""
+    out = []
+    for c in counts:
+        out.append(index % c)
+        index //= c
+    return np.array(out, np.int64)
+
+
+def serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", min_values: int = 3, max_values: int = 5,
+          probe_values: int = 3, walks: int = 2, rel_tol: float = 1e-5) -> ServeResult:
+    """The learned-proposal path for a batch of pairs.
+
+    1. The network proposes a window of the full grid per pair (cgs_proposal_window).
+    2. One persistent launch searches every pair's window (and, on the first pass, a coarse
+       probe of the full grid: full-grid points, so its best bounds the full grid's best).
+    3. A window's best is accepted when it is a local minimum of the window -- on every axis
+       strictly inside the window, or on a window edge that is the grid's edge -- and beats the
+       probe's best.  A best on an inner window edge moves the window to centre on it (at most
+       `walks` times); anything else is searched on the full grid.
+    Each pair's answer is the best point found."""
+    n = int(fixed.shape[0])
+    counts = np.array([int(c) for c in full.getAxisSampleCounts()], np.int64)
+    step = int(getattr(net, "max_batch", n) or n)
+    out = np.concatenate([net.forward(fixed[i:i + step], moving[i:i + step]).cpu().numpy()
+                          for i in range(0, n, step)])
+    windows = [proposal_window(full, out[i], min_values, max_values) for i in range(n)]
+    probe = coarse_grid(full, probe_values)
+    params = np.zeros((n, full.g.dims))
+    costs = np.full(n, np.inf)
+    pcost = np.full(n, np.inf)
+    fallback = np.zeros(n, bool)
+    pending = list(range(n))
+    pts = 0
+    for it in range(walks + 1):
+        if not pending:
+            break
+        grids = [grid_window(full, *windows[i]) for i in pending]
+        idx = list(pending)
+        if it == 0:
+            grids += [probe] * n
+            idx += list(range(n))
+        p, c, v, k = _batch_search(cost, fixed[idx], moving[idx], grids, fixed.device)
+        pts += k
+        if it == 0:
+            pcost = np.where(v[len(pending):], c[len(pending):], np.inf)
+            pp = p[len(pending):]
+        nxt = []
+        for j, i in enumerate(pending):
+            if not v[j]:
+                fallback[i] = True
+                continue
+            if c[j] < costs[i]:
+                params[i], costs[i] = p[j], c[j]
+            first, cnt = windows[i]
+            # the window's best in window indices, recovered from its parameters
+            g = grids[j]
+            lo = np.array([g.g.start[a] for a in range(g.g.dims)], np.float64)
+            res = np.array([g.g.resolution[a] for a in range(g.g.dims)], np.float64)
+            loc = np.where(cnt > 1, np.rint((p[j] - lo) / np.where(res != 0, res, 1.0)), 0).astype(np.int64)
+            on_low = (loc == 0) & (first > 0)
+            on_high = (loc == cnt - 1) & (first + cnt < counts)
+            if not (on_low | on_high).any():
+                if not c[j] < pcost[i] - rel_tol * max(1.0, abs(pcost[i])):
+                    fallback[i] = True
+                continue
+            if it == walks:
+                fallback[i] = True
+                continue
+            centre = first + loc
+            nf = np.clip(centre - (cnt - 1) // 2, 0, counts - cnt)
+            windows[i] = (nf, cnt)
+            nxt.append(i)
+        pending = nxt
+    if fallback.any():
+        fi = np.flatnonzero(fallback)
+        pf, cf, _, k = _batch_search(cost, fixed[fi], moving[fi], [full] * len(fi), fixed.device)
+        pts += k
+        params[fi], costs[fi] = pf, cf
+    better = pcost < costs  # the probe itself can hold the best point found
+    params[better], costs[better] = pp[better], pcost[better]
+    return ServeResult(params, costs, fallback, pts)
+
+
+def corner_error(p_a, p_b, side: int = 256) -> np.ndarray:
+    """Mean distance (px) between the image corners mapped by the homographies of parameter
+    vectors p_a and p_b (centred parametrisation at side / 2), per row."""
+    from .synthetic import homography
+    pa, pb = np.atleast_2d(p_a), np.atleast_2d(p_b)
+    corners = np.array([[0, 0, 1], [side - 1, 0, 1], [0, side - 1, 1], [side - 1, side - 1, 1]], np.float64).T
+    out = []
+    for a, b in zip(pa, pb):
+        qa = homography(a, "centred", side / 2.0, side / 2.0) @ corners
+        qb = homography(b, "centred", side / 2.0, side / 2.0) @ corners
+        qa, qb = qa[:2] / qa[2], qb[:2] / qb[2]
+        out.append(float(np.mean(np.hypot(*(qa - qb)))))
+    return np.array(out)
+
+
+def downsample(x, s: int):
+    """s x s box average of a (n, side, side) CUDA stack (the network's own input rule)."""
+    import torch
+    n, h, w = x.shape
+    return x.reshape(n, h // s, s, w // s, s).mean(dim=(2, 4)).contiguous()
+
+
+def train(net: ProposalNet, fixed, moving, labels_u, epochs: int, batch: int = 256, lr: float = 1e-3,
+          seed: int = 0, log=None) -> list[float]:
+    """Adam on the Laplace loss over (fixed, moving, labels) CUDA tensors; returns per-epoch
+    mean losses."""
+    import torch
+    n = int(fixed.shape[0])
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    lab = torch.as_tensor(np.asarray(labels_u, np.float32), device=fixed.device)
+    hist = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g).to(fixed.device)
+        tot = torch.zeros(1, device=fixed.device)
+        steps = 0
+        for i in range(0, n - batch + 1, batch):
+            ix = perm[i:i + batch]
+            tot += net.train_step(fixed[ix].contiguous(), moving[ix].contiguous(), lab[ix].contiguous(), lr)
+            steps += 1
+        hist.append(float(tot) / max(1, steps))
+        if log:
+            log(f"epoch {ep}: loss {hist[-1]:.4f}")
+    return hist
+
+
+def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, label_side: int = 128,
+               min_values: int = 3, max_values: int = 5, batch: int = 256, checkpoint: str | None = None,
+               variants=None, log=print) -> dict:
+    """The learned-proposal configuration end to end on the current GPU: generate training pairs
+    (256 px), label them with the full 6^8 ZNCC grid on the 2x box-averaged pairs, train, then on
+    held-out 256 px pairs compare the served proposal path with the full grid (the judge):
+    corner error, cost gap, fallback rate and pairs/s of both (CUDA events)."""
+    import json
+    import os
+    import time
+
+    import torch
+    dev = torch.device("cuda")
+    os.makedirs(out_dir, exist_ok=True)
+    t0 = time.time()
+    full_l = full_grid(label_side, 6)
+    lo_l, hi_l = full_l.matrix()[0], full_l.matrix()[1]
+    fs, ms, us = [], [], []
+    s = 256 // label_side
+    chunk = 512
+    t_label = 0.0
+    net = ProposalNet(max_batch=batch, seed=seed)
+    hist, t_train = [float("nan")], 0.0
+    if checkpoint:  # a network trained earlier on the same generator: evaluation only
+        net.load(checkpoint)
+        n_train = 0
+    for i in range(0, n_train, chunk):
+        k = min(chunk, n_train - i)
+        f, m, _ = config4_batch_cached(seed + i, k, dev)
+        fd, md = downsample(f, s), downsample(m, s)
+        torch.cuda.synchronize()
+        tl = time.time()
+        p, _ = grid_argmins(fd, md, full_l)
+        t_label += time.time() - tl
+        fs.append(fd)
+        ms.append(md)
+        us.append(to_units(p, lo_l, hi_l).astype(np.float32))
+        log(f"labelled {i + k}/{n_train} ({t_label:.0f} s in the grid search)")
+    ckpt = checkpoint
+    if n_train:
+        F, M, U = torch.cat(fs), torch.cat(ms), np.concatenate(us)
+        del fs, ms
+        np.save(os.path.join(out_dir, "labels.npy"), U)
+        tt = time.time()
+        hist = train(net, F, M, U, epochs=epochs, batch=batch, lr=1e-3, seed=seed, log=log)
+        torch.cuda.synchronize()
+        t_train = time.time() - tt
+        ckpt = os.path.join(out_dir, "proposal_net.npz")
+        net.save(ckpt)
+        del F, M
+    # evaluation at 256 px: the full grid (the judge) once, then each serving variant
+    full = full_grid(256, 6)
+    fe, me, gte = config4_batch_cached(seed + 10 ** 7, n_eval, dev)
+    ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev[0].record()
+    truth, tcost = grid_argmins(fe, me, full)
+    ev[1].record()
+    torch.cuda.synchronize()
+    t_full = ev[0].elapsed_time(ev[1]) / 1e3
+    # how often the label resolution's argmin is the evaluation resolution's
+    lab_e, _ = grid_argmins(downsample(fe, 256 // label_side), downsample(me, 256 // label_side), full_l)
+    same = np.all(np.isclose(to_units(lab_e, lo_l, hi_l), to_units(truth, full.matrix()[0], full.matrix()[1]),
+                             atol=1e-4), axis=1)
+    res = {"n_train": n_train, "n_eval": n_eval, "epochs": epochs, "label_side": label_side,
+           "label_matches_eval_argmin": float(same.mean()), "loss_first": hist[0], "loss_last": hist[-1],
+           "label_seconds": round(t_label, 1), "train_seconds": round(t_train, 1),
+           "full_grid_pairs_per_s": n_eval / t_full,
+           "gt_corner_error_full_grid_px": float(corner_error(truth, gte.numpy(), 256).mean()),
+           "checkpoint": ckpt, "variants": []}
+    for (mn, mx, walks) in variants or [(min_values, max_values, 2)]:
+        serve(net, fe[:8], me[:8], full, min_values=mn, max_values=mx, walks=walks)  # warm-up
+        ev[0].record()
+        r = serve(net, fe, me, full, min_values=mn, max_values=mx, walks=walks)
+        ev[1].record()
+        torch.cuda.synchronize()
+        t_serve = ev[0].elapsed_time(ev[1]) / 1e3
+        err = corner_error(r.params, truth, 256)
+        gap = r.costs - tcost
+        res["variants"].append({
+            "min_values": mn, "max_values": mx, "walks": walks,
+            "proposal_pairs_per_s": n_eval / t_serve, "speedup": t_full / t_serve,
+            "fallback_rate": float(r.fallback.mean()), "corner_error_mean_px": float(err.mean()),
+            "corner_error_p90_px": float(np.percentile(err, 90)), "agree_within_0_5px": float(np.mean(err <= 0.5)),
+            "cost_gap_mean": float(np.mean(gap)), "cost_gap_max": float(np.max(gap)),
+            "points_fraction": r.points / (n_eval * full.numElements()),
+            "gt_corner_error_px": float(corner_error(r.params, gte.numpy(), 256).mean())})
+        log(json.dumps(res["variants"][-1]))
+    res["wall_seconds"] = round(time.time() - t0, 1)
+    with open(os.path.join(out_dir, "proposal_eval.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+    net.close()
+    return res
+
+
+def config4_batch_cached(seed: int, n: int, device):
+    """config4_batch in chunks of at most 256 pairs (bounded generator memory)."""
+    import torch
+    from .synthetic import config4_batch
+    fs, ms, gs = [], [], []
+    for i in range(0, n, 256):
+        f, m, g = config4_batch(seed + i, min(256, n - i), device)
+        fs.append(f)
+        ms.append(m)
+        gs.append(g)
+    return torch.cat(fs), torch.cat(ms), torch.cat(gs)
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train and evaluate the learned proposal (one GPU)")
+    ap.add_argument("--train", type=int, default=8192)
+    ap.add_argument("--eval", type=int, default=512)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--out", default="proposal_run")
+    ap.add_argument("--min-values", type=int, default=3)
+    ap.add_argument("--max-values", type=int, default=5)
+    ap.add_argument("--checkpoint", default=None, help="evaluate this trained network instead of training")
+    ap.add_argument("--variants", default="3,3,2;3,3,6;3,3,10;3,5,2;3,5,6",
+                    help="serving variants min_values,max_values,walks separated by ';'")
+    a = ap.parse_args()
+    vs = [tuple(int(x) for x in v.split(",")) for v in a.variants.split(";") if v]
+    print(json.dumps(experiment(a.train, a.eval, a.epochs, a.seed, a.out, min_values=a.min_values,
+                                max_values=a.max_values, checkpoint=a.checkpoint, variants=vs)))

@@ -203,3 +203,69 @@ def small_pair(seed: int, size: int = 32, count: int = 3, cost: str = "ZNCC", u8
             return np.round(st).astype(np.uint8) if u8 else st.astype(np.float32)
         p.fixed, p.moving = extra(p.fixed), extra(p.moving)
     return p
+
+
+def config4_ranges(side: int = 256):
+    """Grid ranges of the learned-proposal configuration for images of `side` pixels: rotation
+    +-20 deg, scale 0.9-1.1, shear +-0.05, translation +-32 px and perspective +-1e-4 at 256 px
+    (translation scales with the side, perspective inversely)."""
+    f = side / 256.0
+    return _ranges(20, 0.1, 0.05, 32 * f, 1e-4 / f)
+
+
+def config4_batch(seed: int, n: int, device, side: int = 256):
+    """n pairs of the learned-proposal configuration generated on the GPU with torch (training
+    and evaluation data; same distribution as config4(), not the same numbers): 40 blobs with
+    sigma 12-40 px (at 256 px) plus the sinusoid texture, the moving image m(q) = f(H q) for a
+    ground-truth H drawn uniformly in the grid ranges (centred parametrisation), Gaussian noise
+    sigma 2, clipped to [0, 255].  Returns (fixed, moving, gt) as float32 tensors of shapes
+    (n, side, side), (n, side, side), (n, 8)."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(int(seed))
+    u = lambda *shape: torch.rand(*shape, generator=g, dtype=torch.float64)
+    f = side / 256.0
+    lo, hi = config4_ranges(side)
+    lo_t, hi_t = torch.tensor(lo, dtype=torch.float64), torch.tensor(hi, dtype=torch.float64)
+    gt = (lo_t + (hi_t - lo_t) * u(n, 8)).float()
+    cx, cy = u(n, 40) * side, u(n, 40) * side
+    sg = (12 + 28 * u(n, 40)) * f
+    amp = 40 + 160 * u(n, 40)
+    lx, ly = side / 12 + (side / 5 - side / 12) * u(n), side / 12 + (side / 5 - side / 12) * u(n)
+    ph = 2 * math.pi * u(n, 2)
+    noise_seed = int(torch.randint(0, 2 ** 62, (1,), generator=g))
+    dev = torch.device(device)
+    yy, xx = torch.meshgrid(torch.arange(side, device=dev, dtype=torch.float32),
+                            torch.arange(side, device=dev, dtype=torch.float32), indexing="ij")
+    img = torch.zeros((n, side, side), device=dev, dtype=torch.float32)
+    for b in range(40):
+        c_x, c_y = cx[:, b].float().to(dev)[:, None, None], cy[:, b].float().to(dev)[:, None, None]
+        s2 = (2 * sg[:, b] ** 2).float().to(dev)[:, None, None]
+        img += amp[:, b].float().to(dev)[:, None, None] * torch.exp(-((xx - c_x) ** 2 + (yy - c_y) ** 2) / s2)
+    tx = torch.sin(2 * math.pi * xx / lx.float().to(dev)[:, None, None] + ph[:, 0].float().to(dev)[:, None, None])
+    ty = torch.sin(2 * math.pi * yy / ly.float().to(dev)[:, None, None] + ph[:, 1].float().to(dev)[:, None, None])
+    img += 0.2 * 255.0 * 0.5 * (1 + tx * ty)
+    fixed = img.clamp_(0, 255)
+    H = torch.tensor(np.stack([homography(p, "centred", side / 2.0, side / 2.0) for p in gt.numpy()]),
+                     dtype=torch.float32, device=dev)
+    X = H[:, 0, 0, None, None] * xx + H[:, 0, 1, None, None] * yy + H[:, 0, 2, None, None]
+    Y = H[:, 1, 0, None, None] * xx + H[:, 1, 1, None, None] * yy + H[:, 1, 2, None, None]
+    Z = H[:, 2, 0, None, None] * xx + H[:, 2, 1, None, None] * yy + H[:, 2, 2, None, None]
+    x, y = X / Z, Y / Z
+    x0, y0 = torch.floor(x), torch.floor(y)
+    ax, ay = x - x0, y - y0
+    pad = torch.nn.functional.pad(fixed, (1, 1, 1, 1))
+    ix, iy = x0.long() + 1, y0.long() + 1
+    ok = (ix >= 0) & (iy >= 0) & (ix < side + 1) & (iy < side + 1)
+    ixc, iyc = ix.clamp(0, side), iy.clamp(0, side)
+    flat = pad.reshape(n, -1)
+    w2 = side + 2
+
+    def tap(dy, dx):
+        return torch.gather(flat, 1, ((iyc + dy) * w2 + ixc + dx).reshape(n, -1)).reshape(n, side, side)
+
+    m = ((1 - ax) * (1 - ay) * tap(0, 0) + ax * (1 - ay) * tap(0, 1) + (1 - ax) * ay * tap(1, 0) +
+         ax * ay * tap(1, 1))
+    m = torch.where(ok, m, torch.zeros_like(m))
+    gn = torch.Generator(device=dev).manual_seed(noise_seed)
+    m = (m + 2.0 * torch.randn(m.shape, generator=gn, device=dev)).clamp_(0, 255)
+    return fixed.contiguous(), m.contiguous(), gt

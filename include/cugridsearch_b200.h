@@ -96,6 +96,13 @@ typedef struct cgs_options {
  * 0-8), FAST for CGS_COST_ZNCC and CGS_COST_MI.  The scanline functors (6-8) are always exact. */
 #define CGS_FLAG_EXACT_SAMPLES 2
 #define CGS_FLAG_FAST_SAMPLES 4
+/* Where the 2x2 bilinear taps come from.  QUAD: a staged copy of the moving image that holds
+ * each pixel's footprint as one 16-byte element (4x the moving image in scratch); TEXTURE:
+ * texture gathers (scalar loads for MI).  Default: quads for the fast sampling path of every
+ * cost but MI, texture otherwise (the faster choice measured on B200).  Results are identical;
+ * only speed and scratch size differ. */
+#define CGS_FLAG_QUAD_TAPS 8
+#define CGS_FLAG_TEXTURE_TAPS 16
 
 /* Argmin of a search: the lowest cost, ties broken by the lowest grid index.  NaN and
  * +inf costs never win (the reference compares with '<', cudaTensor.cuh:256 and
@@ -182,6 +189,62 @@ cgs_status cgs_covariance(const cgs_grid *grid, const float *costs, uint64_t n, 
 cgs_status cgs_mi_histogram(const cgs_image *moving, const cgs_image *fixed, const float params[8], int32_t bins,
                             uint32_t *hist, cgs_stream_t stream);
 
+/* Coarse-to-fine search, the loop of the reference's driver (src/gpu/cudaGridSearch_main_mi.cu:
+ * 312-363): `depth` searches, each followed by re-centring every axis on the argmin's value p
+ * with the reference's float arithmetic -- start' = p - (end - start) / 4, then
+ * end' = p + (end - start') / 4 using the updated start -- the counts set again and the grid
+ * updated as its setters do.  levels (host, nullable, depth entries) receives each level's
+ * argmin; final_grid (host, nullable) the last level's grid.  A level without a finite cost
+ * ends the loop (its argmin, valid = 0, fills the remaining entries).  Synchronous: every level
+ * waits for the previous argmin. */
+cgs_status cgs_search_refine(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
+                             const cgs_options *options, int32_t depth, cgs_argmin *levels, cgs_grid *final_grid,
+                             cgs_stream_t stream);
+
+/* ---------------------------------------------------------------- after the search
+ *
+ * parametersToHomography (src/gpu/cudaImageFunctions.cuh:216-252; centred = 1, centre (cx, cy),
+ * normalised by h33) or the uncentred form inlined in averageAbsoluteDifference
+ * (src/gpu/cudaErrorFunctions.cuh:42-57; centred = 0): H = {h11, h12, h13, h21, h22, h23, h31,
+ * h32} of parameters [theta, sx, sy, shear, tx, ty, kx, ky], in the reference's float
+ * operation order (host). */
+cgs_status cgs_homography(const float params[8], float cx, float cy, int32_t centred, float H[8]);
+
+/* transformImage (src/gpu/cudaImageFunctions.cuh:40-60), one thread per output pixel: for
+ * every (x, y) in [0, cols) x [0, rows) the inverse map of H gives a point of `in`; where it
+ * lies inside `in`, out(y, x, c) = in.valueAt_bilinear(point, c) converted to the pixel type,
+ * elsewhere `out` keeps its value.  in and out are DEVICE images of one pixel type and channel
+ * count; out is written (its data pointer is treated as writable).  The arithmetic is the
+ * reference's device build (fused multiply-adds where nvcc forms them). */
+cgs_status cgs_transform_image(const float H[8], int32_t rows, int32_t cols, const cgs_image *in, cgs_image *out,
+                               cgs_stream_t stream);
+
+/* fuseAlignedImages (src/gpu/cudaImageFunctions.cuh:62-112): the 3-channel overlay, channel 0
+ * the moving image under estimated_H, 1 the reference image as it is, 2 the moving image under
+ * true_H, each sampled at `channel` of its source; pixels that map outside keep their value.
+ * fused is a DEVICE 3-channel image of the sources' pixel type (written). */
+cgs_status cgs_fuse_aligned(const float estimated_H[8], const float true_H[8], const cgs_image *reference,
+                            const cgs_image *moving, cgs_image *fused, int32_t channel, cgs_stream_t stream);
+
+/* ---------------------------------------------------------------- before the search
+ *
+ * CudaImage::filter (include/cudaTensor.cuh:578-597 -> filterProcess, include/cudaTensorKernels.cuh:
+ * 353-394): per pixel, channels whose action is 1 (FILTER) receive the correlation with `filter`
+ * (a DEVICE single-channel float image, centred at ((h - 1) / 2, (w - 1) / 2)), taps outside
+ * the image taking the centre pixel's value; channels whose action is 0 (COPY) are copied.  As
+ * in the reference one running sum serves all FILTER channels of a pixel (it is not reset per
+ * channel) and is converted to the pixel type.  actions: host array, one entry per channel.
+ * in and out: DEVICE images of one shape and type (out is written). */
+cgs_status cgs_filter_image(const cgs_image *filter, const cgs_image *in, cgs_image *out, const int32_t actions[],
+                            cgs_stream_t stream);
+
+/* Intensity quantisation of a uint8 image in place (transformPixel,
+ * src/cpu/multispectral_ImageMatcher.cu:411-428): each sample read as a signed char v,
+ * v = (int)(v / mod), v = (int)(v * mod), stored back modulo 256.  The reference's threads at
+ * x == width or y == height (bound check '>') also rewrite the next row's first pixel or write
+ * past the image; here every pixel is quantised exactly once. */
+cgs_status cgs_quantize_image(cgs_image *img, float mod, cgs_stream_t stream);
+
 /* ---------------------------------------------------------------- batched search
  *
  * Many image pairs of uneven sizes, each with its own grid and cost, evaluated by ONE
@@ -256,6 +319,60 @@ cgs_status cgs_search_batched(const cgs_pair *pairs, int32_t n, const cgs_batch_
 
 /* Autotunes a temporary batch of these pairs and returns the best plan. */
 cgs_status cgs_autotune(const cgs_pair *pairs, int32_t n, int32_t sample_points, cgs_batch_plan *best);
+
+/* ---------------------------------------------------------------- learned proposal network
+ *
+ * No counterpart in the reference.  A small CNN looks at an image pair and predicts where the
+ * grid search's argmin lies: for each of the 8 parameters a centre c (grid-range units: -1 at
+ * the grid's start, +1 at its end) and a log-radius s (the same units).  It is trained on pairs
+ * whose labels are this library's own grid-search argmins, by this library's kernels (BF16
+ * tensor-core implicit-GEMM convolutions with FP32 accumulation, FP32 MLP, Adam); the proposal
+ * then narrows the grid (cgs_proposal_window, cgs_grid_window) and the full grid stays the fallback.
+ *
+ * Architecture: the pair box-averaged to 128 x 128 (fixed, moving as 2 channels), five 3x3
+ * stride-2 convolutions with ReLU (32-64-128-128-256 channels), global average pool, dense
+ * 256 -> 128 (ReLU) -> 16 (c[0..7], s[0..7]).  Loss: mean over samples and parameters of the
+ * Laplace negative log-likelihood |c - y| e^-s + s, s clamped to [-6, 4]. */
+typedef struct cgs_net cgs_net; /* opaque: parameters, Adam state, activations of one batch */
+
+/* Number of FP32 parameters (the flat layout of get/set_params). */
+int64_t cgs_net_param_count(void);
+
+/* Allocates a network for batches of up to max_batch pairs, He-initialised from seed. */
+cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **net);
+cgs_status cgs_net_destroy(cgs_net *net);
+
+/* Copies of the flat FP32 parameters / the gradients of the last backward (host buffers of
+ * cgs_net_param_count() floats).  Synchronising. */
+cgs_status cgs_net_get_params(const cgs_net *net, float *host_params);
+cgs_status cgs_net_set_params(cgs_net *net, const float *host_params);
+cgs_status cgs_net_get_grads(const cgs_net *net, float *host_grads);
+
+/* Forward pass on n pairs: fixed and moving are DEVICE stacks of n single-channel float images
+ * of side x side pixels (side a multiple of 128; box-averaged to 128).  out (nullable) is a
+ * DEVICE array of n x 16 floats.  Asynchronous on stream. */
+cgs_status cgs_net_forward(cgs_net *net, const float *fixed, const float *moving, int32_t n, int32_t side, float *out,
+                           cgs_stream_t stream);
+
+/* Backward pass of the last forward: labels is a DEVICE array of n x 8 targets (grid-range
+ * units); gradients land in the network; loss (nullable DEVICE float) receives the mean loss. */
+cgs_status cgs_net_backward(cgs_net *net, const float *labels, float *loss, cgs_stream_t stream);
+
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected) with learning rate lr. */
+cgs_status cgs_net_adam_step(cgs_net *net, float lr, cgs_stream_t stream);
+
+/* A window of a grid by index: on axis a the count[a] consecutive values from index first[a].
+ * Its values are the grid's own (decoded as CudaGrid::indexToGridPoint does), so a search of
+ * the window evaluates points of the grid.  `grid` needs integral counts. */
+cgs_status cgs_grid_window(const cgs_grid *grid, const int32_t first[8], const int32_t count[8], cgs_grid *window);
+
+/* The window a proposal implies on `full` (integral counts): per axis the values centred on the
+ * value nearest the proposed centre c that hold every value within the radius e^s of c
+ * (half-width floor(radius / resolution + 1/2)), widened to min_values or narrowed to
+ * max_values (both odd) and shifted to stay inside the grid.  out is the network's 16 outputs
+ * of the pair (host); first/count receive the window (axes past dims: 0 / 1). */
+cgs_status cgs_proposal_window(const cgs_grid *full, const float out[16], int32_t min_values, int32_t max_values,
+                               int32_t first[8], int32_t count[8]);
 
 /* Synchronous convenience: cgs_search on `stream`, then copies the argmin to *host_result. */
 cgs_status cgs_search_sync(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,

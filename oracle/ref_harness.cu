@@ -109,6 +109,49 @@ static int device_grid_points(const float *start, const float *end, const float 
     return rc;
 }
 
+/* The reference's transformImage and fuseAlignedImages (cudaImageFunctions.cuh:40-112) on the
+ * DEVICE, launched <<<1,1>>> as its drivers launch them and compiled with nvcc's default flags.
+ * pix: 0 = float, 1 = uint8_t; channels 1 or 3.  Every pointer is a device pointer; the
+ * input buffers must hold (H + 1) * W * C + C elements (zeros after the image), the reach of
+ * the reference's bilinear taps.  Returns 0, 1 on a CUDA error, 2 on unsupported arguments. */
+template <typename P, uint8_t C>
+static int transform_t(const float *H, int rows, int cols, const void *in, int ih, int iw, void *out, int oh, int ow) {
+    nv_ext::Vec<float, 8> h(H);
+    CudaImage<P, C> I(ih, iw), O(oh, ow);
+    I.data() = (P *)in;
+    O.data() = (P *)out;
+    transformImage<P, 8, C><<<1, 1>>>(h, rows, cols, I, O);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
+template <typename P, uint8_t C>
+static int fuse_t(const float *He, const float *Ht, const void *ref, int rh, int rw, const void *mov, int mh, int mw,
+                  void *fused, int fh, int fw, int ch) {
+    nv_ext::Vec<float, 8> he(He), ht(Ht);
+    CudaImage<P, C> R(rh, rw), M(mh, mw);
+    CudaImage<P, 3> F(fh, fw);
+    R.data() = (P *)ref;
+    M.data() = (P *)mov;
+    F.data() = (P *)fused;
+    fuseAlignedImages<P, 8, C><<<1, 1>>>(he, ht, R, M, F, ch);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
+/* The reference's CudaImage::filter (filterProcess on the DEVICE, include/cudaTensor.cuh:578-597).
+ * Device pointers; actions one per channel (0 COPY, 1 FILTER). */
+template <typename P, uint32_t C>
+static int filter_t(const float *filt, int fh, int fw, const void *in, int h, int w, void *out, const int *actions) {
+    CudaImage<float, 1> F(fh, fw);
+    F.data() = (float *)filt;
+    CudaImage<P, C> I(h, w), O(h, w);
+    I.data() = (P *)in;
+    O.data() = (P *)out;
+    CHANNEL_ACTION acts[C];
+    for (uint32_t c = 0; c < C; c++) acts[c] = actions[c] ? FILTER : COPY;
+    I.filter(F, O, acts);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
 extern "C" {
 
 /* One reference functor evaluation. pix: 0 = float, 1 = uint8_t, 2 = double, 3 = uint16_t. */
@@ -183,6 +226,31 @@ int cgsref_search(int cost, int dims, const float *start, const float *res, cons
 }
 
 int cgsref_max_threads(void) { return omp_get_max_threads(); }
+
+int cgsref_transform_image(int pix, int channels, const float *H, int rows, int cols, const void *in, int ih, int iw,
+                           void *out, int oh, int ow) {
+    if (pix == 0 && channels == 1) return transform_t<float, 1>(H, rows, cols, in, ih, iw, out, oh, ow);
+    if (pix == 0 && channels == 3) return transform_t<float, 3>(H, rows, cols, in, ih, iw, out, oh, ow);
+    if (pix == 1 && channels == 1) return transform_t<uint8_t, 1>(H, rows, cols, in, ih, iw, out, oh, ow);
+    if (pix == 1 && channels == 3) return transform_t<uint8_t, 3>(H, rows, cols, in, ih, iw, out, oh, ow);
+    return 2;
+}
+
+int cgsref_filter(int pix, int channels, const float *filt, int fh, int fw, const void *in, int h, int w, void *out,
+                  const int *actions) {
+    if (pix == 0 && channels == 1) return filter_t<float, 1>(filt, fh, fw, in, h, w, out, actions);
+    if (pix == 1 && channels == 1) return filter_t<uint8_t, 1>(filt, fh, fw, in, h, w, out, actions);
+    if (pix == 1 && channels == 3) return filter_t<uint8_t, 3>(filt, fh, fw, in, h, w, out, actions);
+    return 2;
+}
+
+int cgsref_fuse_aligned(int pix, int channels, const float *He, const float *Ht, const void *ref, int rh, int rw,
+                        const void *mov, int mh, int mw, void *fused, int fh, int fw, int ch) {
+    if (pix == 0 && channels == 1) return fuse_t<float, 1>(He, Ht, ref, rh, rw, mov, mh, mw, fused, fh, fw, ch);
+    if (pix == 1 && channels == 1) return fuse_t<uint8_t, 1>(He, Ht, ref, rh, rw, mov, mh, mw, fused, fh, fw, ch);
+    if (pix == 1 && channels == 3) return fuse_t<uint8_t, 3>(He, Ht, ref, rh, rw, mov, mh, mw, fused, fh, fw, ch);
+    return 2;
+}
 
 int cgsref_device_grid_points(int dims, const float *start, const float *end, const float *count, const int64_t *idx,
                               int n, float *out, float *matrix) {

@@ -149,3 +149,22 @@ def test_batch_struct_layout():
         got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     assert got == [C.sizeof(abi.CgsPair), abi.CgsPair.costs.offset, abi.CgsPair.result.offset,
                    C.sizeof(abi.CgsBatchPlan), C.sizeof(abi.CgsTuneEntry)]
+
+
+def test_homography_matches_reference_host_build(lib):
+    """cgs_homography against the reference's parametersToHomography built for the host."""
+    import cugridsearch_b200 as cgs
+    if not O.have_ref():
+        pytest.skip("reference harness not built")
+    R = O.ref()
+    R.cgsref_params_to_h.restype = None
+    R.cgsref_params_to_h.argtypes = [C.POINTER(C.c_float), C.c_float, C.c_float, C.POINTER(C.c_float)]
+    rng = np.random.default_rng(9)
+    for _ in range(200):
+        p = np.array([rng.uniform(-0.5, 0.5), rng.uniform(0.8, 1.2), rng.uniform(0.8, 1.2), rng.uniform(-0.1, 0.1),
+                      rng.uniform(-30, 30), rng.uniform(-30, 30), rng.uniform(-1e-3, 1e-3), rng.uniform(-1e-3, 1e-3)],
+                     np.float32)
+        cx, cy = float(rng.integers(8, 300)) / 2, float(rng.integers(8, 300)) / 2
+        ref = (C.c_float * 8)()
+        R.cgsref_params_to_h((C.c_float * 8)(*p), cx, cy, ref)
+        np.testing.assert_array_equal(cgs.homography(p, cx, cy), np.array(list(ref), np.float32))

@@ -200,3 +200,19 @@ def test_fast_path_decisions_match_exact_path(cuda, lib, cost):
         np.testing.assert_array_equal(np.isfinite(cf), fin)
         assert np.max(np.abs(cf[fin] - ce[fin]) / np.maximum(np.abs(ce[fin]), 1.0)) < 2e-6
     assert rf.index == re.index or abs(rf.cost - re.cost) <= 2e-6 * max(1.0, abs(re.cost))
+
+
+@pytest.mark.parametrize("fast", [True, False])
+@pytest.mark.parametrize("cost", ["SAD_AVG", "SAD_AVG_H", "SQD_REF", "NCC_REF", "ZNCC", "MI"])
+def test_quad_taps_identical(cuda, lib, cost, fast):
+    """Taps from pre-gathered quads (CGS_FLAG_QUAD_TAPS) give the same costs, bit for bit, as
+    texture gathers or scalar loads, in both sampling modes, on ragged three-channel images
+    (the W - 1 < x < W alias and the last-row pad) -- and the oracle's tolerance holds."""
+    channels = 1 if cost == "SAD_AVG_H" else 3
+    pair = S.small_pair(29, size=29, count=3, cost=cost, msize=23, channels=channels)
+    base, c0, _ = _gpu_search(cuda, pair, cost, exact_samples=not fast, quad_taps=False)
+    res, c1, grid = _gpu_search(cuda, pair, cost, exact_samples=not fast, quad_taps=True)
+    np.testing.assert_array_equal(c1.view(np.uint32), c0.view(np.uint32))
+    assert res.index == base.index
+    c32, c64 = _oracle(pair, cost)
+    _check(res, c1, c32, c64, cost, grid)

@@ -1,0 +1,183 @@
+"""CPU tests of the learned proposal: the float64 reference network's gradients against finite
+differences (so it can serve as the GPU kernels' gradient oracle), the window rule and grid
+windows (cgs_proposal_window, cgs_grid_window: host functions of the library), the coarse probe
+and corner errors."""
+import numpy as np
+import pytest
+import torch
+
+import oracle.proposal_ref as R
+
+
+@pytest.fixture(scope="module")
+def small_net():
+    rng = np.random.default_rng(5)
+    off, total = R.layout()
+    p = np.zeros(total)
+    for l in range(5):
+        o, (co, kp) = off[f"w{l}"]
+        w = rng.normal(0, np.sqrt(2.0 / (9 * R.CIN[l])), (co, kp))
+        w[:, 9 * R.CIN[l]:] = 0
+        p[o:o + co * kp] = w.ravel()
+        o, (cb,) = off[f"b{l}"]
+        p[o:o + cb] = rng.normal(0, 0.05, cb)
+    for name, sd in (("fc1w", np.sqrt(2.0 / 256)), ("fc1b", 0.05), ("fc2w", 0.1), ("fc2b", 0.1)):
+        o, sh = off[name]
+        p[o:o + int(np.prod(sh))] = rng.normal(0, sd, int(np.prod(sh)))
+    fixed = rng.uniform(0, 255, (2, 128, 128))
+    moving = rng.uniform(0, 255, (2, 128, 128))
+    labels = rng.uniform(-1, 1, (2, 8))
+    return p, fixed, moving, labels
+
+
+def test_reference_gradients_match_finite_differences(small_net):
+    p, fixed, moving, labels = small_net
+    _, L, g = R.loss_and_grads(p, fixed, moving, labels, bf16=False)
+    x = R.net_input(fixed, moving, bf16=False)
+    lab = torch.from_numpy(labels)
+    off, _ = R.layout()
+    rng = np.random.default_rng(1)
+    picks = []
+    for name in ("w0", "b0", "w2", "w4", "b4", "fc1w", "fc2w", "fc2b"):
+        o, sh = off[name]
+        n = int(np.prod(sh))
+        idx = [i for i in rng.integers(0, n, 40) if name != "w0" or (i % sh[1]) < 18][:4]
+        picks += [o + int(i) for i in idx]
+    for i in picks:
+        h = 1e-5
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        lp = float(R.loss(R.forward(torch.from_numpy(pp), x, bf16=False), lab))
+        lm = float(R.loss(R.forward(torch.from_numpy(pm), x, bf16=False), lab))
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_reference_padding_weights_have_zero_gradient(small_net):
+    p, fixed, moving, labels = small_net
+    _, _, g = R.loss_and_grads(p, fixed, moving, labels, bf16=True)
+    off, _ = R.layout()
+    o, (co, kp) = off["w0"]
+    assert np.all(g[o:o + co * kp].reshape(co, kp)[:, 18:] == 0)
+
+
+def _full():
+    from cugridsearch_b200 import proposal as P
+    return P.full_grid(256, 6)
+
+
+def test_proposal_window_rule(lib):
+    """Windows hold the proposed centre's nearest value, span the radius (clamped to
+    [min_values, max_values]) and stay inside the grid."""
+    from cugridsearch_b200 import proposal as P
+    full = _full()
+    rng = np.random.default_rng(3)
+    n = 6
+    for _ in range(200):
+        out = np.concatenate([rng.uniform(-1.2, 1.2, 8), rng.uniform(-7, 5, 8)]).astype(np.float32)
+        for mn, mx in ((1, 1), (1, 5), (3, 5), (3, 3), (5, 5)):
+            first, cnt = P.proposal_window(full, out, mn, mx)
+            assert np.all(cnt >= mn) and np.all(cnt <= mx) and np.all(cnt % 2 == 1)
+            assert np.all(first >= 0) and np.all(first + cnt <= n)
+            ic = np.floor((np.clip(out[:8], -1, 1) + 1) * 0.5 * (n - 1) + 0.5).astype(int)
+            assert np.all((first <= ic) & (ic <= first + cnt - 1))
+            w = np.floor(np.exp(np.clip(out[8:], -6, 4)) * 0.5 * (n - 1) + 0.5)
+            want = np.clip(2 * w + 1, mn, mx)
+            np.testing.assert_array_equal(cnt, want)
+
+
+def test_grid_window_values_are_full_grid_values(lib):
+    from cugridsearch_b200 import proposal as P
+    full = _full()
+    counts = [int(c) for c in full.getAxisSampleCounts()]
+    inc = np.cumprod([1] + counts[:-1])
+    rng = np.random.default_rng(8)
+    for _ in range(20):
+        cnt = rng.integers(1, 6, 8)
+        first = np.array([rng.integers(0, 6 - c + 1) for c in cnt])
+        g = P.grid_window(full, first, cnt)
+        np.testing.assert_array_equal(g.getAxisSampleCounts(), cnt.astype(np.float32))
+        winc = np.cumprod([1] + list(cnt[:-1]))
+        for a in range(8):
+            for j in range(cnt[a]):
+                v = float(g.getGridPoint(int(j * winc[a]))[a])
+                ref = float(full.getGridPoint(int((first[a] + j) * inc[a]))[a])
+                assert abs(v - ref) <= 2e-6 * max(1.0, abs(ref)), (a, j, v, ref)
+    with pytest.raises(Exception):
+        P.grid_window(full, np.full(8, 4), np.full(8, 3))  # past the last value
+
+
+def test_coarse_probe_is_full_grid_points(lib):
+    from cugridsearch_b200 import proposal as P
+    full = _full()
+    probe = P.coarse_grid(full, 3)
+    np.testing.assert_array_equal(probe.getAxisSampleCounts(), np.full(8, 3.0))
+    counts = [int(c) for c in full.getAxisSampleCounts()]
+    inc = np.cumprod([1] + counts[:-1])
+    for a in range(8):
+        for j, i in enumerate((0, 2, 4)):
+            v = float(probe.getGridPoint(int(j * 3 ** a))[a])
+            assert abs(v - float(full.getGridPoint(int(i * inc[a]))[a])) <= 2e-6 * max(1.0, abs(v))
+
+
+def test_corner_error():
+    from cugridsearch_b200 import proposal as P
+    p = np.array([0.1, 1.0, 1.0, 0.0, 3.0, -2.0, 0.0, 0.0])
+    assert P.corner_error(p, p)[0] == 0.0
+    q = p.copy()
+    q[4] += 1.0  # one pixel of translation moves every corner by one pixel
+    assert abs(P.corner_error(p, q)[0] - 1.0) < 1e-9
+
+
+def _oracle_batch_search(cost, fixed, moving, grids, device):
+    """serve()'s batch search, done by the CPU oracle (FP32 reference sums, lowest index)."""
+    import oracle as O
+    ps, cs, vs, pts = [], [], [], 0
+    for i, g in enumerate(grids):
+        m = g.matrix()
+        og = O.make_grid(m[0], m[1], m[3])
+        c32, _ = O.search(cost, og, O.Image(moving[i].numpy()[:, :, None]), O.Image(fixed[i].numpy()[:, :, None]),
+                          f64=False)
+        c = np.where(np.isfinite(c32), c32, np.inf)
+        k = int(np.argmin(c))
+        ps.append(O.grid_point(og, k)[: g.g.dims].astype(np.float64))
+        cs.append(float(c[k]))
+        vs.append(bool(np.isfinite(c[k])))
+        pts += g.numElements()
+    return np.stack(ps), np.array(cs), np.array(vs), pts
+
+
+def test_serve_logic_with_oracle_search(lib, monkeypatch):
+    """The serving logic (windows, walks, local-minimum check, probe, fallback) with the searches
+    done by the oracle: aimed proposals return the full grid's argmins without a fallback, off-target
+    ones walk or fall back and still return them, and the points evaluated are counted."""
+    from cugridsearch_b200 import proposal as P
+    from cugridsearch_b200 import synthetic as S
+    monkeypatch.setattr(P, "_batch_search", _oracle_batch_search)
+    pairs = [S.small_pair(500 + i, size=16, count=4, cost="ZNCC") for i in range(3)]
+    fixed = torch.from_numpy(np.stack([p.fixed[:, :, 0] for p in pairs]))
+    moving = torch.from_numpy(np.stack([p.moving[:, :, 0] for p in pairs]))
+    from cugridsearch_b200 import CudaGrid
+    full = CudaGrid.from_ranges(*pairs[0].grid_args())
+    truth, tcost, _, _ = _oracle_batch_search("ZNCC", fixed, moving, [full] * 3, None)
+    lo, hi = full.matrix()[0], full.matrix()[1]
+
+    class Net:
+        def __init__(self, out):
+            self.out = out
+
+        def forward(self, f, m):
+            return torch.from_numpy(self.out)
+
+    u = P.to_units(truth, lo, hi)
+    aimed = np.concatenate([u, np.full((3, 8), -5.0)], 1).astype(np.float32)
+    r = P.serve(Net(aimed), fixed, moving, full, min_values=3, max_values=3)
+    assert not r.fallback.any()
+    np.testing.assert_allclose(r.params, truth, atol=1e-6)
+    # off by one lattice step on every axis: a walk (or the fallback) recovers the argmins
+    step = 2.0 / 3.0
+    off = np.concatenate([np.clip(u + step, -1, 1), np.full((3, 8), -5.0)], 1).astype(np.float32)
+    r2 = P.serve(Net(off), fixed, moving, full, min_values=3, max_values=3, walks=3)
+    np.testing.assert_allclose(r2.costs, tcost, rtol=1e-6, atol=1e-7)
+    assert r2.points > r.points
