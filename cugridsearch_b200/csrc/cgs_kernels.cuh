@@ -59,7 +59,7 @@ struct SearchParams {
     unsigned int *status;
     const float *vmax;   // max |moving pixel| (from the staging kernel)
     cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
-    const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y, x+1), (y+1, x), (y+1, x+1)}
+    const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y+1, x), (y, x+1), (y+1, x+1)}
     int32_t quad_pitch;           // quads per row
     int64_t quad_plane;           // quads per channel
     const float *row_table;       // calcMIAlt's row values (the float recurrence row += 1/(H_f-1))
@@ -455,6 +455,8 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
     constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
     constexpr bool kTexTaps = (TAPS == kTapsTexture);
     constexpr int PSTEP = BSPLIT ? NW * 32 : 32;  // pixel stride of a lane
+    constexpr bool kPacked = (G % 2 == 0);         // fast path on pairs of points (FP32x2)
+    constexpr int GP = kPacked ? G / 2 : 1;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int fw = p.fix.w, fh = p.fix.h;
@@ -505,6 +507,20 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
         mg[g].hy = 0.5f - gy;
         if (lane == 0) my_slots[g] = ExactSlot{kc.P, kc.Q, kc.R, kc.S, kc.T, kc.U, gx, gy, rt, kc.B, kc.C2, kc.D2, 0.0f};
     }
+
+    // packed per-task constants of the fast path (pairs of points)
+    float2 A2[GP], C12[GP], D12[GP];
+    if constexpr (kPacked) {
+#pragma unroll
+        for (int h = 0; h < GP; h++) {
+            A2[h] = make_float2(fm[2 * h].A, fm[2 * h + 1].A);
+            C12[h] = make_float2(fm[2 * h].C1, fm[2 * h + 1].C1);
+            D12[h] = make_float2(fm[2 * h].D1, fm[2 * h + 1].D1);
+        }
+    }
+    const float2 nhw2 = make_float2(-hw, -hw), nhh2 = make_float2(-hh, -hh);
+    const float2 magic2 = make_float2(kMagic, kMagic), nmagic2 = make_float2(-kMagic, -kMagic);
+    const float2 minus1 = make_float2(-1.0f, -1.0f);
 
     float *tot = sm.acc + warp * G * NA * 32 + lane;
     int cnt[G];
@@ -634,15 +650,29 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             int xx = pstart, yy = 0;
             while (xx >= fw) { xx -= fw; yy++; }
             float xf = (float)xx;
+            // per-row terms of the map; with an even G they are kept as pairs of points for the
+            // packed FP32x2 operations below (each component rounds as the scalar operation)
             float byw[G], byx[G], byy[G];
+            float2 byw2[GP], byx2[GP], byy2[GP];
             auto set_row = [&](int yrow) {
                 const float yf = (float)(r0 + yrow);
+                if constexpr (kPacked) {
+                    const float2 yf2 = make_float2(yf, yf);
 #pragma unroll
-                for (int g = 0; g < G; g++) {
-                    const RowTerms rt = my_slots[g].rt;
-                    byw[g] = fmaf(rt.B, yf, rt.PQ);
-                    byx[g] = fmaf(rt.C2, yf, rt.RS);
-                    byy[g] = fmaf(rt.D2, yf, rt.TU);
+                    for (int h = 0; h < GP; h++) {
+                        const RowTerms ra = my_slots[2 * h].rt, rb = my_slots[2 * h + 1].rt;
+                        byw2[h] = __ffma2_rn(make_float2(ra.B, rb.B), yf2, make_float2(ra.PQ, rb.PQ));
+                        byx2[h] = __ffma2_rn(make_float2(ra.C2, rb.C2), yf2, make_float2(ra.RS, rb.RS));
+                        byy2[h] = __ffma2_rn(make_float2(ra.D2, rb.D2), yf2, make_float2(ra.TU, rb.TU));
+                    }
+                } else {
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const RowTerms rt = my_slots[g].rt;
+                        byw[g] = fmaf(rt.B, yf, rt.PQ);
+                        byx[g] = fmaf(rt.C2, yf, rt.RS);
+                        byy[g] = fmaf(rt.D2, yf, rt.TU);
+                    }
                 }
             };
             set_row(yy);
@@ -650,53 +680,96 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                 FixTerms ft[C];
 #pragma unroll
                 for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B);
-                // 1. fast coordinates and decisions of all G points (independent chains)
+                // 1. fast coordinates, decisions and cell coordinates of all G points
+                //    (independent chains): tx = floor + 1.5 * 2^23 (round-down add), fx = floor,
+                //    ax = fraction
                 bool fin[G], amb[G];
-                float mxs[G], mys[G];
-#pragma unroll
-                for (int g = 0; g < G; g++) {
-                    const float w = fmaf(fm[g].A, xf, byw[g]);
-                    const float X = fmaf(fm[g].C1, xf, byx[g]);
-                    const float Y = fmaf(fm[g].D1, xf, byy[g]);
-                    const float rw = rcp_approx(w);
-                    mxs[g] = X * rw;
-                    mys[g] = Y * rw;
-                    const float dx = fabsf(mxs[g] - hw), dy = fabsf(mys[g] - hh);
+                float mxs[G], mys[G], txs[G], tys[G], fxs[G], fys[G], axs[G], ays[G];
+                auto decide = [&](int g, float dx, float dy) {
                     fin[g] = (dx < fm[g].li_x) & (dy < fm[g].li_y);              // clearly inside
                     amb[g] = !fin[g] & !((dx > fm[g].lo_x) | (dy > fm[g].lo_y)); // undecided: exact path
+                };
+                if constexpr (kPacked) {
+                    const float2 xf2 = make_float2(xf, xf);
+#pragma unroll
+                    for (int h = 0; h < GP; h++) {
+                        const int g = 2 * h;
+                        const float2 w = __ffma2_rn(A2[h], xf2, byw2[h]);
+                        const float2 X = __ffma2_rn(C12[h], xf2, byx2[h]);
+                        const float2 Y = __ffma2_rn(D12[h], xf2, byy2[h]);
+                        const float2 rw = make_float2(rcp_approx(w.x), rcp_approx(w.y));
+                        const float2 mx = __fmul2_rn(X, rw), my = __fmul2_rn(Y, rw);
+                        const float2 dx = __fadd2_rn(mx, nhw2), dy = __fadd2_rn(my, nhh2);
+                        decide(g, fabsf(dx.x), fabsf(dy.x));
+                        decide(g + 1, fabsf(dx.y), fabsf(dy.y));
+                        const float2 tx = __fadd2_rd(mx, magic2), ty = __fadd2_rd(my, magic2);
+                        const float2 fx = __fadd2_rn(tx, nmagic2), fy = __fadd2_rn(ty, nmagic2);
+                        const float2 ax = __ffma2_rn(fx, minus1, mx), ay = __ffma2_rn(fy, minus1, my);
+                        mxs[g] = mx.x; mxs[g + 1] = mx.y; mys[g] = my.x; mys[g + 1] = my.y;
+                        txs[g] = tx.x; txs[g + 1] = tx.y; tys[g] = ty.x; tys[g + 1] = ty.y;
+                        fxs[g] = fx.x; fxs[g + 1] = fx.y; fys[g] = fy.x; fys[g + 1] = fy.y;
+                        axs[g] = ax.x; axs[g + 1] = ax.y; ays[g] = ay.x; ays[g + 1] = ay.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const float w = fmaf(fm[g].A, xf, byw[g]);
+                        const float X = fmaf(fm[g].C1, xf, byx[g]);
+                        const float Y = fmaf(fm[g].D1, xf, byy[g]);
+                        const float rw = rcp_approx(w);
+                        mxs[g] = X * rw;
+                        mys[g] = Y * rw;
+                        decide(g, fabsf(mxs[g] - hw), fabsf(mys[g] - hh));
+                        txs[g] = __fadd_rd(mxs[g], kMagic);
+                        tys[g] = __fadd_rd(mys[g], kMagic);
+                        fxs[g] = txs[g] - kMagic;
+                        fys[g] = tys[g] - kMagic;
+                        axs[g] = mxs[g] - fxs[g];
+                        ays[g] = mys[g] - fys[g];
+                    }
                 }
-                // 2. taps of all G points: one texture gather returns the 2x2 footprint; the
+                // 2. taps of all G points.  Texture: one gather returns the 2x2 footprint; the
                 //    gather coordinate is the footprint's centre, (floor + 1) in texel units, so
-                //    the texture unit's fixed-point coordinate rounding cannot change the cell.
-                //    Points not clearly inside read zeros from the border.
+                //    the texture unit's fixed-point coordinate rounding cannot change the cell;
+                //    points not clearly inside read zeros from the border.  Quads: one 16-byte
+                //    load of the footprint (points not clearly inside read quad 0, unused).
                 float v[G][C];
 #pragma unroll
                 for (int g = 0; g < G; g++) {
-                    const float tx = __fadd_rd(mxs[g], kMagic), ty = __fadd_rd(mys[g], kMagic);
-                    const float fx = tx - kMagic, fy = ty - kMagic;
-                    const float ax = mxs[g] - fx, ay = mys[g] - fy;
+                    const float tx = txs[g], ty = tys[g], fx = fxs[g], fy = fys[g], ax = axs[g], ay = ays[g];
                     const float u = fin[g] ? fx + 1.0f : -4.0f;
                     const int ix = __float_as_int(tx) - kMagicBits, iy = __float_as_int(ty) - kMagicBits;
                     const int base = fin[g] ? ix + mpitch * iy : 0;
                     const int qbase = fin[g] ? ix + qpitch * iy : 0;
 #pragma unroll
                     for (int c = 0; c < C; c++) {
-                        float v00, v01, v10, v11;
-                        if constexpr (kTexTaps) {
-                            const float4 t4 = tex2Dgather<float4>(mtex, u, fy + 1.0f + (float)c * mrows, 0);
-                            // gather order: x = (i0, j1), y = (i1, j1), z = (i1, j0), w = (i0, j0)
-                            v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
-                        } else if constexpr (TAPS == kTapsQuad) {
+                        float v00, v01, v10, v11, d0, d1;
+                        if constexpr (TAPS == kTapsQuad) {
+                            // quad = {left column (v00, v10), right column (v01, v11)}: the column
+                            // differences and the two row lerps as packed pairs
                             const float4 q4 = __ldg(mquad + c * qplane + qbase);
-                            v00 = q4.x; v01 = q4.y; v10 = q4.z; v11 = q4.w;
+                            v00 = q4.x; v10 = q4.y; v01 = q4.z; v11 = q4.w;
+                            const float2 left = make_float2(q4.x, q4.y), right = make_float2(q4.z, q4.w);
+                            const float2 dd = __ffma2_rn(left, minus1, right);         // (v01 - v00, v11 - v10)
+                            const float2 tb = __ffma2_rn(make_float2(ax, ax), dd, left);  // (top, bottom)
+                            d0 = dd.x;
+                            d1 = dd.y;
+                            v[g][c] = fmaf(ay, tb.y - tb.x, tb.x);
                         } else {
-                            const float *pl = mdata + c * mplane + base;
-                            v00 = __ldg(pl); v01 = __ldg(pl + 1);
-                            v10 = __ldg(pl + mpitch); v11 = __ldg(pl + mpitch + 1);
+                            if constexpr (kTexTaps) {
+                                const float4 t4 = tex2Dgather<float4>(mtex, u, fy + 1.0f + (float)c * mrows, 0);
+                                // gather order: x = (i0, j1), y = (i1, j1), z = (i1, j0), w = (i0, j0)
+                                v00 = t4.w; v01 = t4.z; v10 = t4.x; v11 = t4.y;
+                            } else {
+                                const float *pl = mdata + c * mplane + base;
+                                v00 = __ldg(pl); v01 = __ldg(pl + 1);
+                                v10 = __ldg(pl + mpitch); v11 = __ldg(pl + mpitch + 1);
+                            }
+                            d0 = v01 - v00;
+                            d1 = v11 - v10;
+                            const float top = fmaf(ax, d0, v00), bot = fmaf(ax, d1, v10);
+                            v[g][c] = fmaf(ay, bot - top, top);
                         }
-                        const float d0 = v01 - v00, d1 = v11 - v10;
-                        const float top = fmaf(ax, d0, v00), bot = fmaf(ax, d1, v10);
-                        v[g][c] = fmaf(ay, bot - top, top);
                         if constexpr (kMI) {
                             // the bin is exact unless the sample could lie across a bin edge (or the
                             // coordinate across a cell edge) from the reference's sample

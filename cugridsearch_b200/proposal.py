@@ -182,13 +182,16 @@ def full_grid(side: int = 256, values: int = 6):
     return CudaGrid.from_ranges([float(v) for v in lo], [float(v) for v in hi], [values] * 8)
 
 
-def _batch_search(cost, fixed, moving, grids, device):
+def _batch_search(cost, fixed, moving, grids, device, dump=None):
     """One persistent launch over pairs i with grid grids[i]: (params (n, 8), costs (n,),
-    valid (n,), points evaluated)."""
+    valid (n,), points evaluated).  dump: indices of the pairs whose whole cost arrays are
+    wanted; they are then returned as a fifth element (dict index -> numpy array)."""
     import torch
     from . import Batch, BatchPair, CudaImage, read_result, result_buffer
     res = [result_buffer(device) for _ in grids]
-    pairs = [BatchPair(cost, CudaImage(moving[i]), CudaImage(fixed[i]), g, res[i]) for i, g in enumerate(grids)]
+    dumps = {i: torch.empty(grids[i].numElements(), dtype=torch.float32, device=device) for i in (dump or ())}
+    pairs = [BatchPair(cost, CudaImage(moving[i]), CudaImage(fixed[i]), g, res[i], dumps.get(i))
+             for i, g in enumerate(grids)]
     with Batch(pairs) as b:
         b.launch()
         torch.cuda.synchronize(device)
@@ -196,7 +199,10 @@ def _batch_search(cost, fixed, moving, grids, device):
     params = np.stack([o.params for o in out]).astype(np.float64)
     costs = np.array([o.cost for o in out], np.float64)
     valid = np.array([o.valid and o.status == 0 for o in out])
-    return params, costs, valid, int(sum(g.numElements() for g in grids))
+    pts = int(sum(g.numElements() for g in grids))
+    if dump is not None:
+        return params, costs, valid, pts, {i: t.cpu().numpy() for i, t in dumps.items()}
+    return params, costs, valid, pts
 
 
 def grid_argmins(fixed, moving, grid, cost: str = "ZNCC", chunk: int = 256):
@@ -222,77 +228,92 @@ def _axis_indices(index: int, counts) -> np.ndarray:
 
 
 def serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", min_values: int = 3, max_values: int = 5,
-          probe_values: int = 3, walks: int = 2, rel_tol: float = 1e-5) -> ServeResult:
+          probe_values: int = 3, walks: int = 6, starts: int = 2) -> ServeResult:
     """The learned-proposal path for a batch of pairs.
 
-    1. The network proposes a window of the full grid per pair (cgs_proposal_window).
-    2. One persistent launch searches every pair's window (and, on the first pass, a coarse
-       probe of the full grid: full-grid points, so its best bounds the full grid's best).
-    3. A window's best is accepted when it is a local minimum of the window -- on every axis
-       strictly inside the window, or on a window edge that is the grid's edge -- and beats the
-       probe's best.  A best on an inner window edge moves the window to centre on it (at most
-       `walks` times); anything else is searched on the full grid.
-    Each pair's answer is the best point found."""
+    1. The network proposes a window of the full grid per pair (cgs_proposal_window).  One
+       persistent launch searches every pair's window and a coarse probe of the full grid
+       (full-grid points, so its best bounds the full grid's best from above).
+    2. With starts = k > 1, k - 1 more walkers per pair start from min_values-wide windows
+       centred on the probe's k - 1 best points.
+    3. A walker whose window's best lies strictly inside the window on every axis (or on a
+       window edge that is the grid's edge) stops there: a certified local minimum of the grid.
+       A best on an inner window edge moves the window to centre on it, at most `walks` times.
+       Every pass over the pending walkers of all pairs is one persistent launch.
+    4. A pair's answer is the best certified point (or the probe's best, if lower); a pair
+       without any certified point is searched on the full grid (the fallback)."""
     n = int(fixed.shape[0])
+    d = full.g.dims
     counts = np.array([int(c) for c in full.getAxisSampleCounts()], np.int64)
     step = int(getattr(net, "max_batch", n) or n)
     out = np.concatenate([net.forward(fixed[i:i + step], moving[i:i + step]).cpu().numpy()
                           for i in range(0, n, step)])
-    windows = [proposal_window(full, out[i], min_values, max_values) for i in range(n)]
     probe = coarse_grid(full, probe_values)
-    params = np.zeros((n, full.g.dims))
+    params = np.zeros((n, d))
     costs = np.full(n, np.inf)
-    pcost = np.full(n, np.inf)
-    fallback = np.zeros(n, bool)
-    pending = list(range(n))
+    certified = np.zeros(n, bool)
+    # walkers: [pair, first, count, walks left]
+    walkers = [[i, *proposal_window(full, out[i], min_values, max_values), walks] for i in range(n)]
+    start = np.array([full.g.start[a] for a in range(d)], np.float64)
+    fres = np.array([full.g.resolution[a] for a in range(d)], np.float64)
     pts = 0
-    for it in range(walks + 1):
-        if not pending:
-            break
-        grids = [grid_window(full, *windows[i]) for i in pending]
-        idx = list(pending)
-        if it == 0:
+    first_pass = True
+    while walkers:
+        grids = [grid_window(full, w[1], w[2]) for w in walkers]
+        idx = [w[0] for w in walkers]
+        if first_pass:
             grids += [probe] * n
             idx += list(range(n))
-        p, c, v, k = _batch_search(cost, fixed[idx], moving[idx], grids, fixed.device)
+        nw = len(walkers)
+        if first_pass and starts > 1:
+            p, c, v, k, dumps = _batch_search(cost, fixed[idx], moving[idx], grids, fixed.device,
+                                              dump=range(nw, nw + n))
+        else:
+            p, c, v, k = _batch_search(cost, fixed[idx], moving[idx], grids, fixed.device)
         pts += k
-        if it == 0:
-            pcost = np.where(v[len(pending):], c[len(pending):], np.inf)
-            pp = p[len(pending):]
         nxt = []
-        for j, i in enumerate(pending):
+        for j in range(nw):
+            i, first, cnt, left = walkers[j]
             if not v[j]:
-                fallback[i] = True
                 continue
             if c[j] < costs[i]:
                 params[i], costs[i] = p[j], c[j]
-            first, cnt = windows[i]
-            # the window's best in window indices, recovered from its parameters
             g = grids[j]
-            lo = np.array([g.g.start[a] for a in range(g.g.dims)], np.float64)
-            res = np.array([g.g.resolution[a] for a in range(g.g.dims)], np.float64)
+            lo = np.array([g.g.start[a] for a in range(d)], np.float64)
+            res = np.array([g.g.resolution[a] for a in range(d)], np.float64)
             loc = np.where(cnt > 1, np.rint((p[j] - lo) / np.where(res != 0, res, 1.0)), 0).astype(np.int64)
-            on_low = (loc == 0) & (first > 0)
-            on_high = (loc == cnt - 1) & (first + cnt < counts)
-            if not (on_low | on_high).any():
-                if not c[j] < pcost[i] - rel_tol * max(1.0, abs(pcost[i])):
-                    fallback[i] = True
-                continue
-            if it == walks:
-                fallback[i] = True
-                continue
-            centre = first + loc
-            nf = np.clip(centre - (cnt - 1) // 2, 0, counts - cnt)
-            windows[i] = (nf, cnt)
-            nxt.append(i)
-        pending = nxt
+            on_edge = ((loc == 0) & (first > 0)) | ((loc == cnt - 1) & (first + cnt < counts))
+            if not on_edge.any():
+                certified[i] = True
+            elif left > 0:
+                nxt.append([i, np.clip(first + loc - (cnt - 1) // 2, 0, counts - cnt), cnt, left - 1])
+        if first_pass:
+            pp, pc, pv = p[nw:], c[nw:], v[nw:]
+            for i in range(n):
+                if pv[i] and pc[i] < costs[i]:
+                    params[i], costs[i] = pp[i], pc[i]
+            if starts > 1:
+                # the probe's best points (lowest index first on ties), as full-grid indices
+                width = np.minimum(min_values, counts)
+                pcounts = np.array([int(cc) for cc in probe.getAxisSampleCounts()], np.int64)
+                pstep = np.where(pcounts > 1, (counts - 1) // np.maximum(pcounts - 1, 1), 0)
+                for i in range(n):
+                    pd = dumps[nw + i]
+                    cand = np.where(np.isfinite(pd), pd, np.inf)
+                    order = np.argsort(cand, kind="stable")[: starts - 1]
+                    for q in order:
+                        if not np.isfinite(cand[q]):
+                            break
+                        centre = _axis_indices(int(q), pcounts) * pstep
+                        nxt.append([i, np.clip(centre - (width - 1) // 2, 0, counts - width), width.copy(), walks])
+            first_pass = False
+        walkers = nxt
+    fallback = ~certified
     if fallback.any():
         fi = np.flatnonzero(fallback)
         pf, cf, _, k = _batch_search(cost, fixed[fi], moving[fi], [full] * len(fi), fixed.device)
         pts += k
         params[fi], costs[fi] = pf, cf
-    better = pcost < costs  # the probe itself can hold the best point found
-    params[better], costs[better] = pp[better], pcost[better]
     return ServeResult(params, costs, fallback, pts)
 
 
@@ -343,7 +364,7 @@ def train(net: ProposalNet, fixed, moving, labels_u, epochs: int, batch: int = 2
 
 def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, label_side: int = 128,
                min_values: int = 3, max_values: int = 5, batch: int = 256, checkpoint: str | None = None,
-               variants=None, log=print) -> dict:
+               variants=None, init: str | None = None, log=print) -> dict:
     """The learned-proposal configuration end to end on the current GPU: generate training pairs
     (256 px), label them with the full 6^8 ZNCC grid on the 2x box-averaged pairs, train, then on
     held-out 256 px pairs compare the served proposal path with the full grid (the judge):
@@ -367,6 +388,8 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
     if checkpoint:  # a network trained earlier on the same generator: evaluation only
         net.load(checkpoint)
         n_train = 0
+    elif init:  # start training from these parameters
+        net.load(init)
     for i in range(0, n_train, chunk):
         k = min(chunk, n_train - i)
         f, m, _ = config4_batch_cached(seed + i, k, dev)
@@ -410,17 +433,17 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
            "full_grid_pairs_per_s": n_eval / t_full,
            "gt_corner_error_full_grid_px": float(corner_error(truth, gte.numpy(), 256).mean()),
            "checkpoint": ckpt, "variants": []}
-    for (mn, mx, walks) in variants or [(min_values, max_values, 2)]:
-        serve(net, fe[:8], me[:8], full, min_values=mn, max_values=mx, walks=walks)  # warm-up
+    for (mn, mx, walks, starts) in variants or [(min_values, max_values, 6, 2)]:
+        serve(net, fe[:8], me[:8], full, min_values=mn, max_values=mx, walks=walks, starts=starts)  # warm-up
         ev[0].record()
-        r = serve(net, fe, me, full, min_values=mn, max_values=mx, walks=walks)
+        r = serve(net, fe, me, full, min_values=mn, max_values=mx, walks=walks, starts=starts)
         ev[1].record()
         torch.cuda.synchronize()
         t_serve = ev[0].elapsed_time(ev[1]) / 1e3
         err = corner_error(r.params, truth, 256)
         gap = r.costs - tcost
         res["variants"].append({
-            "min_values": mn, "max_values": mx, "walks": walks,
+            "min_values": mn, "max_values": mx, "walks": walks, "starts": starts,
             "proposal_pairs_per_s": n_eval / t_serve, "speedup": t_full / t_serve,
             "fallback_rate": float(r.fallback.mean()), "corner_error_mean_px": float(err.mean()),
             "corner_error_p90_px": float(np.percentile(err, 90)), "agree_within_0_5px": float(np.mean(err <= 0.5)),
@@ -460,9 +483,12 @@ if __name__ == "__main__":
     ap.add_argument("--min-values", type=int, default=3)
     ap.add_argument("--max-values", type=int, default=5)
     ap.add_argument("--checkpoint", default=None, help="evaluate this trained network instead of training")
-    ap.add_argument("--variants", default="3,3,2;3,3,6;3,3,10;3,5,2;3,5,6",
-                    help="serving variants min_values,max_values,walks separated by ';'")
+    ap.add_argument("--init", default=None, help="start training from this network's parameters")
+    ap.add_argument("--label-side", type=int, default=128, help="image side the labels are searched at")
+    ap.add_argument("--variants", default="3,3,6,1;3,3,6,2;3,5,6,1;3,5,6,2",
+                    help="serving variants min_values,max_values,walks,starts separated by ';'")
     a = ap.parse_args()
     vs = [tuple(int(x) for x in v.split(",")) for v in a.variants.split(";") if v]
-    print(json.dumps(experiment(a.train, a.eval, a.epochs, a.seed, a.out, min_values=a.min_values,
-                                max_values=a.max_values, checkpoint=a.checkpoint, variants=vs)))
+    print(json.dumps(experiment(a.train, a.eval, a.epochs, a.seed, a.out, label_side=a.label_side,
+                                min_values=a.min_values, max_values=a.max_values, checkpoint=a.checkpoint,
+                                variants=vs, init=a.init)))

@@ -152,6 +152,49 @@ static int filter_t(const float *filt, int fh, int fw, const void *in, int h, in
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
 }
 
+/* The reference's own GPU search (CudaGridSearcher::search_by_value -> evaluationKernel_by_value,
+ * src/gpu/cudaGridSearch.cuh:287-314, 736-765) of calcNCC or calcMIAlt, compiled unchanged for
+ * sm_100a, timed with CUDA events around the call.  The kernel also writes result[n] (bound
+ * check '>'), so the result buffer holds n + 1 floats; its bilinear taps reach one row past an
+ * image, so the image buffers hold (H + 1) W + 1 elements, zero after the image. */
+typedef func_byvalue_t<float, float, 8, CudaImage<float, 1>, CudaImage<float, 1>> ref_fn_f32;
+typedef func_byvalue_t<float, float, 8, CudaImage<uint8_t, 1>, CudaImage<uint8_t, 1>> ref_fn_u8;
+__device__ ref_fn_f32 ref_dev_ncc_f32 = calcNCC<float, float, 8, 1, float>;
+__device__ ref_fn_u8 ref_dev_mialt_u8 = calcMIAlt<float, float, 8, 1, uint8_t>;
+
+template <typename P, typename Fn>
+static int gpu_search_t(const Fn &dev_fn, const float *start, const float *end, const float *count, const void *mov,
+                        int mh, int mw, const void *fix, int fh, int fw, float *result, float *ms) {
+    CudaGrid<float, 8> g;
+    if (cudaMalloc(&g.data(), g.bytesSize()) != cudaSuccess) return 1;
+    if (cudaMemset(g.data(), 0, g.bytesSize()) != cudaSuccess) return 1;
+    g.setStartPoint(std::vector<float>(start, start + 8));
+    g.setEndPoint(std::vector<float>(end, end + 8));
+    g.setNumSamples(std::vector<float>(count, count + 8));
+    float counts[8];
+    g.getAxisSampleCounts(counts);
+    CudaTensor<float, 8> values(counts);
+    values.data() = result;
+    CudaImage<P, 1> M(mh, mw), F(fh, fw);
+    M.data() = (P *)mov;
+    F.data() = (P *)fix;
+    Fn h;
+    if (cudaMemcpyFromSymbol(&h, dev_fn, sizeof(Fn)) != cudaSuccess) return 1;
+    CudaGridSearcher<float, float, 8> searcher(g, values);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    searcher.search_by_value(h, M, F);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(g.data());
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
 extern "C" {
 
 /* One reference functor evaluation. pix: 0 = float, 1 = uint8_t, 2 = double, 3 = uint16_t. */
@@ -233,6 +276,16 @@ int cgsref_transform_image(int pix, int channels, const float *H, int rows, int 
     if (pix == 0 && channels == 3) return transform_t<float, 3>(H, rows, cols, in, ih, iw, out, oh, ow);
     if (pix == 1 && channels == 1) return transform_t<uint8_t, 1>(H, rows, cols, in, ih, iw, out, oh, ow);
     if (pix == 1 && channels == 3) return transform_t<uint8_t, 3>(H, rows, cols, in, ih, iw, out, oh, ow);
+    return 2;
+}
+
+/* cost: NCC_REF on float images or MI_ALT on uint8 images (single channel, 8 axes). */
+int cgsref_gpu_search(int cost, const float *start, const float *end, const float *count, const void *mov, int mh,
+                      int mw, const void *fix, int fh, int fw, float *result, float *ms) {
+    if (cost == NCC_REF)
+        return gpu_search_t<float>(ref_dev_ncc_f32, start, end, count, mov, mh, mw, fix, fh, fw, result, ms);
+    if (cost == MI_ALT)
+        return gpu_search_t<uint8_t>(ref_dev_mialt_u8, start, end, count, mov, mh, mw, fix, fh, fw, result, ms);
     return 2;
 }
 

@@ -130,10 +130,10 @@ def test_corner_error():
     assert abs(P.corner_error(p, q)[0] - 1.0) < 1e-9
 
 
-def _oracle_batch_search(cost, fixed, moving, grids, device):
+def _oracle_batch_search(cost, fixed, moving, grids, device, dump=None):
     """serve()'s batch search, done by the CPU oracle (FP32 reference sums, lowest index)."""
     import oracle as O
-    ps, cs, vs, pts = [], [], [], 0
+    ps, cs, vs, pts, dumps = [], [], [], 0, {}
     for i, g in enumerate(grids):
         m = g.matrix()
         og = O.make_grid(m[0], m[1], m[3])
@@ -145,6 +145,10 @@ def _oracle_batch_search(cost, fixed, moving, grids, device):
         cs.append(float(c[k]))
         vs.append(bool(np.isfinite(c[k])))
         pts += g.numElements()
+        if dump is not None and i in dump:
+            dumps[i] = c32
+    if dump is not None:
+        return np.stack(ps), np.array(cs), np.array(vs), pts, dumps
     return np.stack(ps), np.array(cs), np.array(vs), pts
 
 
@@ -161,6 +165,7 @@ def test_serve_logic_with_oracle_search(lib, monkeypatch):
     from cugridsearch_b200 import CudaGrid
     full = CudaGrid.from_ranges(*pairs[0].grid_args())
     truth, tcost, _, _ = _oracle_batch_search("ZNCC", fixed, moving, [full] * 3, None)
+    assert np.all(np.isfinite(tcost))
     lo, hi = full.matrix()[0], full.matrix()[1]
 
     class Net:
@@ -172,12 +177,15 @@ def test_serve_logic_with_oracle_search(lib, monkeypatch):
 
     u = P.to_units(truth, lo, hi)
     aimed = np.concatenate([u, np.full((3, 8), -5.0)], 1).astype(np.float32)
-    r = P.serve(Net(aimed), fixed, moving, full, min_values=3, max_values=3)
+    r = P.serve(Net(aimed), fixed, moving, full, min_values=3, max_values=3, starts=1)
     assert not r.fallback.any()
     np.testing.assert_allclose(r.params, truth, atol=1e-6)
     # off by one lattice step on every axis: a walk (or the fallback) recovers the argmins
     step = 2.0 / 3.0
     off = np.concatenate([np.clip(u + step, -1, 1), np.full((3, 8), -5.0)], 1).astype(np.float32)
-    r2 = P.serve(Net(off), fixed, moving, full, min_values=3, max_values=3, walks=3)
+    r2 = P.serve(Net(off), fixed, moving, full, min_values=3, max_values=3, walks=3, starts=1)
     np.testing.assert_allclose(r2.costs, tcost, rtol=1e-6, atol=1e-7)
-    assert r2.points > r.points
+    assert r2.points > r.points  # the walks cost more than the aimed first pass
+    # more starts (the probe's best points) still return the argmins
+    r3 = P.serve(Net(off), fixed, moving, full, min_values=3, max_values=3, walks=3, starts=3)
+    np.testing.assert_allclose(r3.costs, tcost, rtol=1e-6, atol=1e-7)
