@@ -53,6 +53,22 @@ UNIT = "grid-point evals/s"
 TRAFFIC_BYTES_PER_POINT = None
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest x over the ranks (the job's time is its slowest rank's); x itself alone."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seed(rank: int, base: int) -> int:
+    """Seed of a rank's pair: every rank searches its own pair (weak scaling, replicas)."""
+    return base + rank
+
+
 def _env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -181,8 +197,12 @@ def batch_bench(args):
     rank, world, local = _env_rank()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     t_gen = time.perf_counter()
-    pairs = S.config3_pairs(S.DEFAULT_SEED + rank, n=args.pairs)
+    pairs = S.config3_pairs(rank_seed(rank, S.DEFAULT_SEED), n=args.pairs)
     t_gen = time.perf_counter() - t_gen
     stream = torch.cuda.Stream(device=dev)
     host, dev_imgs, bps, results = [], [], [], []
@@ -227,7 +247,7 @@ def batch_bench(args):
             lat.extend(((t1.astype(np.int64) - base) / 1e6).tolist())
             span.extend(((t1.astype(np.int64) - t0.astype(np.int64)) / 1e6).tolist())
     clocks = clk.summary()
-    ms = statistics.median(times)
+    ms = max_over_ranks(statistics.median(times), world, dev)
     # end to end: images in from pinned host memory, the launch, results out
     res_h = [torch.empty(r.numel(), dtype=torch.uint8).pin_memory() for r in results]
     e2e = []
@@ -249,7 +269,12 @@ def batch_bench(args):
     out = [cgs.read_result(r) for r in results]
     h2d = sum(mh.numel() * mh.element_size() + fh.numel() * fh.element_size() for mh, fh in host)
     batch.close()
-    n = len(pairs)
+    e2e_ms = max_over_ranks(statistics.median(e2e), world, dev)
+    if world > 1:
+        dist.destroy_process_group()
+    n = len(pairs) * world  # every rank runs its own batch (weak scaling)
+    points *= world
+    pixel_evals *= world
     line = {"metric": "pairs/s (batched uneven pairs)", "value": n / (ms / 1e3), "unit": "pairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
@@ -259,7 +284,7 @@ def batch_bench(args):
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "span_p50": float(np.percentile(span, 50)),
                            "definition": "pair finish minus the launch's first task start (globaltimer)"},
-            "e2e": {"value": n / (statistics.median(e2e) / 1e3), "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+            "e2e": {"value": n / (e2e_ms / 1e3), "unit": "pairs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": sum(r.numel() for r in res_h)},
             "gpu_launches": 2 * args.steps,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
@@ -311,12 +336,13 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
+    seed = rank_seed(rank, S.DEFAULT_SEED)
     if args.workload == "mi":
-        pair, cost = S.config2(S.DEFAULT_SEED + rank), "MI"
+        pair, cost = S.config2(seed), "MI"
     elif args.workload == "sad":
-        pair, cost = S.config0(S.DEFAULT_SEED + rank), "SAD_AVG"
+        pair, cost = S.config0(seed), "SAD_AVG"
     else:
-        pair, cost = S.config1(S.DEFAULT_SEED + rank), args.cost
+        pair, cost = S.config1(seed), args.cost
     if args.small:
         pair.count[:] = 3
     stream = torch.cuda.Stream(device=dev)
@@ -363,11 +389,7 @@ def main():
             times.append(e0.elapsed_time(e1))
         barrier()
     clocks = clk.summary()
-    total_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(times), world, dev)
     ms_per_step = total_ms / args.steps
     value = world * n * args.steps / (total_ms / 1e3)
     r = cgs.read_result(res)
@@ -394,11 +416,7 @@ def main():
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     barrier()
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(sum(e2e_ms), world, dev)
     e2e_value = world * n * args.steps / (e2e_total / 1e3)
     h2d = mov_h.numel() * mov_h.element_size() + fix_h.numel() * fix_h.element_size()
     d2h = costs_h.numel() * 4 + res_h.numel()

@@ -250,6 +250,7 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
         Staging st;
         int mi_bins;
         int64_t stage_elems;
+        bool quads = false;
     };
     std::vector<Pending> pend((size_t)n);
     for (int32_t i = 0; i < n; i++) {
@@ -274,7 +275,11 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
     for (int32_t i = 0; i < n; i++) {
         const cgs_pair &q = pairs[i];
         Pending &pd = pend[i];
-        pd.st = staging_layout(q.moving, q.fixed, di.tex_align, di.tex_pitch_align);
+        // ZNCC pairs on the fast sampling path read pre-gathered tap quads, as single searches do
+        const int fl = q.options.flags;
+        pd.quads = q.options.cost == CGS_COST_ZNCC &&
+                   ((fl & CGS_FLAG_QUAD_TAPS) || (!exact_samples(CGS_COST_ZNCC, fl) && !(fl & CGS_FLAG_TEXTURE_TAPS)));
+        pd.st = staging_layout(q.moving, q.fixed, di.tex_align, di.tex_pitch_align, false, false, pd.quads);
         set_chunks(&pd.p, pd.st, 1, q.fixed.height);
         pd.stage_elems = pd.st.mplane + pd.st.fplane;
     }
@@ -367,6 +372,13 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
         p.costs = q.costs;
         p.result = q.result;
         preps[j] = make_prep(&q.moving, &q.fixed, pd.st, sb, mstage, fstage);
+        if (pd.quads) {
+            p.mov_quad = reinterpret_cast<const float4 *>(org + pd.st.quad_off);
+            p.quad_pitch = q.moving.width;
+            p.quad_plane = pd.st.qplane;
+            preps[j].quad_dst = reinterpret_cast<float4 *>(org + pd.st.quad_off);
+            preps[j].qplane = pd.st.qplane;
+        }
         // the staged moving plane as a (W + 1) x (H + 1) texture (point sampling, border 0)
         cudaResourceDesc rd;
         memset(&rd, 0, sizeof(rd));

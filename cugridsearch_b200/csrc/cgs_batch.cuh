@@ -123,7 +123,10 @@ __global__ void __launch_bounds__(NW * 32, batch_min_blocks(G, NW)) batch_kernel
             case CGS_COST_SAD_AVG: ok = run_task<CGS_COST_SAD_AVG, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
             case CGS_COST_SQD_REF: ok = run_task<CGS_COST_SQD_REF, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
             case CGS_COST_NCC_REF: ok = run_task<CGS_COST_NCC_REF, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
-            case CGS_COST_ZNCC: ok = run_task<CGS_COST_ZNCC, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod); break;
+            case CGS_COST_ZNCC:  // quads staged: taps from the pre-gathered quads
+                ok = p.mov_quad ? run_task<CGS_COST_ZNCC, C, G, NW, kTapsQuad, BSPLIT>(p, task, sm, it, prod)
+                                : run_task<CGS_COST_ZNCC, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod);
+                break;
             default:  // CGS_COST_MI: the host admits only batch_cost_supported() costs
                 ok = run_task<CGS_COST_MI, C, G, NW, kTapsLoads, BSPLIT>(p, task, sm, it, prod);
                 break;

@@ -24,8 +24,6 @@
 // pixel of an ill-conditioned homography) is recomputed with the reference's exact
 // operation sequence.
 #pragma once
-#include <type_traits>
-
 #include "cgs_device.cuh"
 #include "../../include/cugridsearch_b200.h"
 
@@ -656,23 +654,8 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             // packed FP32x2 operations below (each component rounds as the scalar operation)
             float byw[G], byx[G], byy[G];
             float2 byw2[GP], byx2[GP], byy2[GP];
-            // Whether every pixel of this lane's row maps clearly inside for every point.  The
-            // exact mapped row is the segment between its exact end points (w keeps its sign
-            // over the image wherever the fast path runs), each fast coordinate lies within half
-            // a guard of the exact one, so fast end points 1.5 guards inside the clearly-inside
-            // box put every fast coordinate of the row inside it.
-            bool row_in = false;
-            auto row_inside = [&](int g, float bw, float bx, float by) -> bool {
-                const float xl = (float)(fw - 1);
-                const float w1 = fmaf(fm[g].A, xl, bw), X1 = fmaf(fm[g].C1, xl, bx), Y1 = fmaf(fm[g].D1, xl, by);
-                const float q0 = rcp_approx(bw), q1 = rcp_approx(w1);
-                const float ex = fm[g].li_x - 1.5f * my_slots[g].gx, ey = fm[g].li_y - 1.5f * my_slots[g].gy;
-                return (fabsf(bx * q0 - hw) < ex) & (fabsf(X1 * q1 - hw) < ex) & (fabsf(by * q0 - hh) < ey) &
-                       (fabsf(Y1 * q1 - hh) < ey);
-            };
             auto set_row = [&](int yrow) {
                 const float yf = (float)(r0 + yrow);
-                bool in = true;
                 if constexpr (kPacked) {
                     const float2 yf2 = make_float2(yf, yf);
 #pragma unroll
@@ -681,8 +664,6 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                         byw2[h] = __ffma2_rn(make_float2(ra.B, rb.B), yf2, make_float2(ra.PQ, rb.PQ));
                         byx2[h] = __ffma2_rn(make_float2(ra.C2, rb.C2), yf2, make_float2(ra.RS, rb.RS));
                         byy2[h] = __ffma2_rn(make_float2(ra.D2, rb.D2), yf2, make_float2(ra.TU, rb.TU));
-                        in &= row_inside(2 * h, byw2[h].x, byx2[h].x, byy2[h].x);
-                        in &= row_inside(2 * h + 1, byw2[h].y, byx2[h].y, byy2[h].y);
                     }
                 } else {
 #pragma unroll
@@ -691,18 +672,11 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                         byw[g] = fmaf(rt.B, yf, rt.PQ);
                         byx[g] = fmaf(rt.C2, yf, rt.RS);
                         byy[g] = fmaf(rt.D2, yf, rt.TU);
-                        in &= row_inside(g, byw[g], byx[g], byy[g]);
                     }
                 }
-                row_in = in;
             };
             set_row(yy);
             while (yy < rows) {
-                // a pixel whose rows (across the warp) are inside for every point skips the
-                // per-sample in/out decisions; its body is compiled for both cases
-                const bool all_in = __all_sync(__activemask(), row_in);
-                auto pixel = [&](auto in_tag) {
-                constexpr bool kIn = decltype(in_tag)::value;
                 FixTerms ft[C];
 #pragma unroll
                 for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B);
@@ -712,13 +686,8 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                 bool fin[G], amb[G];
                 float mxs[G], mys[G], txs[G], tys[G], fxs[G], fys[G], axs[G], ays[G];
                 auto decide = [&](int g, float dx, float dy) {
-                    if constexpr (kIn) {
-                        fin[g] = true;
-                        amb[g] = false;
-                    } else {
-                        fin[g] = (dx < fm[g].li_x) & (dy < fm[g].li_y);              // clearly inside
-                        amb[g] = !fin[g] & !((dx > fm[g].lo_x) | (dy > fm[g].lo_y)); // undecided: exact path
-                    }
+                    fin[g] = (dx < fm[g].li_x) & (dy < fm[g].li_y);              // clearly inside
+                    amb[g] = !fin[g] & !((dx > fm[g].lo_x) | (dy > fm[g].lo_y)); // undecided: exact path
                 };
                 if constexpr (kPacked) {
                     const float2 xf2 = make_float2(xf, xf);
@@ -859,9 +828,6 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                         cnt[g] += C;
                     }
                 }
-                };  // pixel
-                if (all_in) pixel(std::true_type{});
-                else pixel(std::false_type{});
                 xx += PSTEP;
                 xf += (float)PSTEP;
                 if (xx >= fw) {

@@ -260,7 +260,10 @@ typedef struct cgs_pair {
     cgs_grid grid;
     cgs_options options;   /* cost: CGS_COST_SAD_AVG, _SQD_REF, _NCC_REF, _ZNCC or _MI; mi_bins,
                               overlap_gate and flags as for cgs_search.  points_per_warp and
-                              warps_per_block are ignored: the batch plan applies            */
+                              warps_per_block are ignored: the batch plan applies.  Taps:
+                              ZNCC pairs follow cgs_search's choice (quads on the fast
+                              sampling path unless CGS_FLAG_TEXTURE_TAPS); the other costs
+                              read texture gathers (MI: scalar loads), whatever the flags   */
     float *costs;          /* nullable DEVICE dump of this pair's grid (as cgs_search)       */
     cgs_argmin *result;    /* DEVICE result of this pair                                     */
 } cgs_pair;
