@@ -48,9 +48,12 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS["ncc"]
 METRIC = "homography evals/s"
 UNIT = "grid-point evals/s"
-# DRAM bytes (read + write) of search_kernel per grid point, from the ncu capture summarised in
-# profiles/search_kernel_zncc_256.md (small-grid capture scaled by grid points).
-TRAFFIC_BYTES_PER_POINT = None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one search_kernel launch on the
+# full-size workload, from a one-pass ncu capture of `bench.py --no-cpu-baseline --steps 1
+# --warmup 3` (the default ncc workload, ZNCC with the default taps): 2.05 MB read (images and
+# staging, once), 512 B written (the 6.7 MB cost dump stays in the 126 MB L2 while the kernel
+# runs).  Measured for that configuration only; the others report null.
+TRAFFIC_BYTES_PER_LAUNCH = {"ncc": 2050000 + 512}
 
 
 def max_over_ranks(x: float, world: int, device) -> float:
@@ -429,7 +432,8 @@ def main():
     peak = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4),
-                "traffic": (TRAFFIC_BYTES_PER_POINT * n if TRAFFIC_BYTES_PER_POINT else None),
+                "traffic": (TRAFFIC_BYTES_PER_LAUNCH.get(args.workload)
+                            if cost == "ZNCC" and not args.small and args.taps == "auto" else None),
                 "peak_source": "nominal FP32 FMA rate: SMs x 128 lanes x 2 flops x max SM clock "
                                "(MEASURED_PEAKS.json holds HBM and bf16 tensor peaks only)",
                 "flops_per_pixel_eval": FLOPS_PER_PIXEL_EVAL.get(cost, 36),

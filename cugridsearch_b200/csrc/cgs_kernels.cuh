@@ -59,7 +59,7 @@ struct SearchParams {
     unsigned int *status;
     const float *vmax;   // max |moving pixel| (from the staging kernel)
     cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
-    const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y+1, x), (y, x+1), (y+1, x+1)}
+    const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y+1, x), (y, x+1) - (y, x), (y+1, x+1) - (y+1, x)}
     int32_t quad_pitch;           // quads per row
     int64_t quad_plane;           // quads per channel
     const float *row_table;       // calcMIAlt's row values (the float recurrence row += 1/(H_f-1))
@@ -743,18 +743,21 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                     const int qbase = fin[g] ? ix + qpitch * iy : 0;
 #pragma unroll
                     for (int c = 0; c < C; c++) {
-                        float v00, v01, v10, v11, d0, d1;
+                        float v00, v01, v10, v11, d0, d1, dy;  // dy: bound of the column differences
                         if constexpr (TAPS == kTapsQuad) {
-                            // quad = {left column (v00, v10), right column (v01, v11)}: the column
-                            // differences and the two row lerps as packed pairs
+                            // quad = {left column (v00, v10), its differences to the right column
+                            // (v01 - v00, v11 - v10), rounded once as here}: the two row lerps as
+                            // one packed pair
                             const float4 q4 = __ldg(mquad + c * qplane + qbase);
-                            v00 = q4.x; v10 = q4.y; v01 = q4.z; v11 = q4.w;
-                            const float2 left = make_float2(q4.x, q4.y), right = make_float2(q4.z, q4.w);
-                            const float2 dd = __ffma2_rn(left, minus1, right);         // (v01 - v00, v11 - v10)
+                            v00 = q4.x; v10 = q4.y; d0 = q4.z; d1 = q4.w;
+                            const float2 left = make_float2(q4.x, q4.y), dd = make_float2(q4.z, q4.w);
                             const float2 tb = __ffma2_rn(make_float2(ax, ax), dd, left);  // (top, bottom)
-                            d0 = dd.x;
-                            d1 = dd.y;
                             v[g][c] = fmaf(ay, tb.y - tb.x, tb.x);
+                            if constexpr (kMI) {
+                                // |v11 - v01| <= |v10 - v00| + |v11 - v10| + |v01 - v00|; the factor
+                                // covers the roundings of the differences and of this sum
+                                dy = (fabsf(v10 - v00) + fabsf(d0) + fabsf(d1)) * (1.0f + 0x1p-20f);
+                            }
                         } else {
                             if constexpr (kTexTaps) {
                                 const float4 t4 = tex2Dgather<float4>(mtex, u, fy + 1.0f + (float)c * mrows, 0);
@@ -769,6 +772,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                             d1 = v11 - v10;
                             const float top = fmaf(ax, d0, v00), bot = fmaf(ax, d1, v10);
                             v[g][c] = fmaf(ay, bot - top, top);
+                            if constexpr (kMI) dy = fmaxf(fabsf(v10 - v00), fabsf(v11 - v01));
                         }
                         if constexpr (kMI) {
                             // the bin is exact unless the sample could lie across a bin edge (or the
@@ -776,8 +780,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                             const float t = v[g][c] * sB;
                             const float fr = t - floorf(t);
                             const float Dx = fmaxf(fabsf(d0), fabsf(d1));
-                            const float Dy = fmaxf(fabsf(v10 - v00), fabsf(v11 - v01));
-                            const float gb = fmaf(Dy, mg[g].sgy, fmaf(Dx, mg[g].sgx, gv0));
+                            const float gb = fmaf(dy, mg[g].sgy, fmaf(Dx, mg[g].sgx, gv0));
                             const bool near = (fabsf(fr - 0.5f) > 0.5f - gb) | (fabsf(ax - 0.5f) > mg[g].hx) |
                                               (fabsf(ay - 0.5f) > mg[g].hy);
                             if (fin[g] & near) {

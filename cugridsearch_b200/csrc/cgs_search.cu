@@ -226,9 +226,10 @@ __device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int6
         q.fix_dst[i] = v;
     }
     if (q.quad_dst) {
-        // tap quads of the staged moving plane, left column then right column:
-        // {P(y, x), P(y + 1, x), P(y, x + 1), P(y + 1, x + 1)} with P the padded plane (column W =
-        // the next row's pixel 0, row H = 0)
+        // tap quads of the staged moving plane, the left column and the FP32 differences to the
+        // right column: {P(y, x), P(y + 1, x), P(y, x + 1) - P(y, x), P(y + 1, x + 1) - P(y + 1, x)}
+        // with P the padded plane (column W = the next row's pixel 0, row H = 0); the search
+        // kernel's bilinear step takes the differences as they are
         const int64_t qtot = q.qplane * q.c;
         auto P = [&](int c, int64_t y, int64_t x) -> float {
             if (y >= q.mh) return 0.0f;
@@ -239,7 +240,8 @@ __device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int6
             const int c = (int)(i / q.qplane);
             const int64_t e = i - (int64_t)c * q.qplane;
             const int64_t y = e / q.mw, x = e - y * q.mw;
-            q.quad_dst[i] = make_float4(P(c, y, x), P(c, y + 1, x), P(c, y, x + 1), P(c, y + 1, x + 1));
+            const float v00 = P(c, y, x), v10 = P(c, y + 1, x);
+            q.quad_dst[i] = make_float4(v00, v10, P(c, y, x + 1) - v00, P(c, y + 1, x + 1) - v10);
         }
     }
     if (q.row_table && tid == 0) {
