@@ -126,15 +126,16 @@ static cgs_status plan_shape(const cgs_batch &b, const cgs_batch_plan &pl, uint3
     if (!plan_valid(pl)) return fail(CGS_ERROR_INVALID_VALUE, "batch plan: points_per_warp 1/2/4/8, warps_per_block 4/8/16, block_split 0/1");
     const int G = pl.points_per_warp, NW = pl.warps_per_block;
     const bool bs = pl.block_split != 0;
-    const uint32_t ppt = (uint32_t)(bs ? G : G * NW);
     size_t acc = 0;
     sh->tasks.assign(b.n, 0u);
     uint64_t total = 0;
     for (uint32_t i = 0; i < b.n; i++) {
+        const int gi = batch_pair_points(b.params[i].cost, G);  // this pair's points per warp
+        const uint32_t ppt = (uint32_t)(bs ? gi : gi * NW);     // points per task
         const uint32_t pts = cap ? std::min(cap, b.params[i].n) : b.params[i].n;
         sh->tasks[i] = (pts + ppt - 1) / ppt;
         total += sh->tasks[i];
-        acc = std::max(acc, acc_bytes(b.params[i].cost, G, NW, bs, b.mi_bins[i]));
+        acc = std::max(acc, acc_bytes(b.params[i].cost, gi, NW, bs, b.mi_bins[i]));
     }
     if (total >= kEndTask) return fail(CGS_ERROR_GRID_TOO_LARGE, "batch has too many tasks for this plan");
     sh->total = (uint32_t)total;

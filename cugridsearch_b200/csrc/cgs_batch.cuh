@@ -89,6 +89,13 @@ __host__ __device__ constexpr int batch_min_blocks(int G, int NW) {
     return ((G >= 8 ? 8 : 16) / NW) < 1 ? 1 : (G >= 8 ? 8 : 16) / NW;
 }
 
+// Points per warp of a pair under a plan of G: MI pairs take at most 2 (their histograms, one
+// per point and warp, would not fit in shared memory at more), the other costs take the plan's
+// G.  A cost's values do not depend on its points per warp.
+__host__ __device__ constexpr int batch_pair_points(int cost, int G) {
+    return cost == CGS_COST_MI ? (G < 2 ? G : 2) : G;
+}
+
 // Costs the batch kernel evaluates (each pair picks one).
 __host__ __device__ constexpr bool batch_cost_supported(int cost) {
     return cost == CGS_COST_SAD_AVG || cost == CGS_COST_SQD_REF || cost == CGS_COST_NCC_REF ||
@@ -127,9 +134,11 @@ __global__ void __launch_bounds__(NW * 32, batch_min_blocks(G, NW)) batch_kernel
                 ok = p.mov_quad ? run_task<CGS_COST_ZNCC, C, G, NW, kTapsQuad, BSPLIT>(p, task, sm, it, prod)
                                 : run_task<CGS_COST_ZNCC, C, G, NW, kTapsTexture, BSPLIT>(p, task, sm, it, prod);
                 break;
-            default:  // CGS_COST_MI: the host admits only batch_cost_supported() costs
-                ok = run_task<CGS_COST_MI, C, G, NW, kTapsLoads, BSPLIT>(p, task, sm, it, prod);
+            default: {  // CGS_COST_MI: the host admits only batch_cost_supported() costs
+                constexpr int GM = batch_pair_points(CGS_COST_MI, G);
+                ok = run_task<CGS_COST_MI, C, GM, NW, kTapsLoads, BSPLIT>(p, task, sm, it, prod);
                 break;
+            }
         }
         if (!ok) {
             if (threadIdx.x == 0) {

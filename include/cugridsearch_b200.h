@@ -270,7 +270,8 @@ typedef struct cgs_pair {
 
 /* Launch plan of the batch kernel (one for the whole launch). */
 typedef struct cgs_batch_plan {
-    int32_t points_per_warp; /* 1, 2, 4 or 8 grid points evaluated together by a warp          */
+    int32_t points_per_warp; /* 1, 2, 4 or 8 grid points evaluated together by a warp; MI pairs
+                                take at most 2 (their per-warp histograms fill shared memory) */
     int32_t warps_per_block; /* 4, 8 or 16: blocks of 128, 256 or 512 threads                 */
     int32_t block_split;     /* 0: each warp owns its points and sweeps every pixel for them; MI
                                 histograms are private per warp.  1: a block's warps share its

@@ -125,16 +125,18 @@ def test_overlap_gate(cuda, lib, cost):
 
 @pytest.mark.parametrize("cost", ["SAD_AVG", "ZNCC", "MI"])
 def test_order_and_tiling_do_not_change_results(cuda, lib, cost):
-    """Locality order vs the reference order, and every points-per-warp setting, give
-    bit-identical costs (each point's sums are formed the same way wherever it runs)."""
+    """Locality order vs the reference order, and every points-per-warp and warps-per-block
+    setting, give bit-identical costs (each point's sums are formed the same way wherever it
+    runs)."""
     pair = S.small_pair(17, size=32, count=3, cost=cost)
     base, c0, _ = _gpu_search(cuda, pair, cost, natural_order=True)
     for g in (1, 2, 4):
         if cost == "MI" and g == 4:
             continue
-        r, c, _ = _gpu_search(cuda, pair, cost, points_per_warp=g)
-        np.testing.assert_array_equal(c, c0)
-        assert r.index == base.index and r.cost == base.cost
+        for nw in (8, 16):
+            r, c, _ = _gpu_search(cuda, pair, cost, points_per_warp=g, warps_per_block=nw)
+            np.testing.assert_array_equal(c, c0)
+            assert r.index == base.index and r.cost == base.cost
 
 
 def test_repeatable(cuda, lib):
