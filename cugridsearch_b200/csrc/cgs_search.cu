@@ -991,7 +991,10 @@ static char *g_static_ptr[64] = {};
 
 // The device address of g_static_scratch on the current device.  In host code the array's
 // name stands for a host-side shadow, not a device address, so it is looked up once per
-// device with cudaGetSymbolAddress while that device is current.
+// device with cudaGetSymbolAddress while that device is current.  The address is kept for the
+// life of the process: after cudaDeviceReset (or any teardown of the device's primary context)
+// the module is loaded again and may be placed elsewhere, so this entry point must not be used
+// across a device reset.
 static cgs_status static_scratch(int dev, char **out) {
     if (dev < 0 || dev >= 64) return fail(CGS_ERROR_NO_DEVICE, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_static_mu);
@@ -1032,6 +1035,10 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
     const cgs_options o = *options;
     const int cost = o.cost;
     const int C = fix->channels;
+    if (is_scanline(cost))
+        return fail(CGS_ERROR_UNSUPPORTED,
+                    "cgs_search_noalloc runs the pixel-loop costs only; the scanline functors (SQD_ALT, NCC_ALT, "
+                    "MI_ALT) need cgs_search");
     // fixed tuning: the plan's MI shape, else 4 points per warp and 16 warps per CTA
     Plan pl;
     const void *kfn = nullptr;

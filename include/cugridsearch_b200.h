@@ -163,7 +163,12 @@ cgs_status cgs_argmin_f32(const float *values, uint64_t n, cgs_argmin *result, c
  *   - all calls on a device share the array, so calls that overlap on the GPU (on different
  *     streams, or from different host threads) race: serialise them;
  *   - points_per_warp / warps_per_block are ignored (4 points per warp, 16 warps; MI keeps its
- *     own shape). */
+ *     own shape);
+ *   - it runs the pixel-loop costs (SAD_AVG, SAD_AVG_H, SAD_SUM_T, SAD_SUM_T_REF, SQD_REF,
+ *     NCC_REF, ZNCC, MI) on 1- and 3-channel images; the scanline functors (SQD_ALT, NCC_ALT,
+ *     MI_ALT) and other channel counts return CGS_ERROR_UNSUPPORTED;
+ *   - the array's device address is kept from the first call on a device, so the entry point
+ *     must not be used across a device reset (cudaDeviceReset). */
 cgs_status cgs_search_noalloc(const cgs_image *moving, const cgs_image *fixed, const cgs_grid *grid,
                               const cgs_options *options, float *costs, cgs_argmin *result, cgs_stream_t stream);
 

@@ -25,7 +25,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libcgs_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcgs_ref.so")
-REF_SRC = os.environ.get("CGS_REFERENCE_DIR", "/root/reference")
+# The reference checkout, when this machine has one: named by the caller (build(ref_dir=...)) or
+# by CGS_REFERENCE_DIR; there is no default location.
+REF_SRC = os.environ.get("CGS_REFERENCE_DIR", "")
 
 COSTS = {
     "SAD_AVG": 0, "SAD_AVG_H": 1, "SAD_SUM_T": 2, "SAD_SUM_T_REF": 3, "SQD_REF": 4,
@@ -52,13 +54,13 @@ class OgGrid(C.Structure):
                 ("resolution", C.c_float * 8), ("count", C.c_float * 8)]
 
 
-def build(ref: bool | None = None) -> None:
-    """Build the oracle (and the reference harness when the checkout is present)."""
+def build(ref_dir: str | None = None) -> None:
+    """Build the oracle, and the reference harness when a reference checkout is given
+    (``ref_dir``, else CGS_REFERENCE_DIR) and present."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref is None:
-        ref = os.path.isdir(os.path.join(REF_SRC, "src", "gpu"))
-    if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
+    ref_dir = ref_dir or REF_SRC
+    if ref_dir and os.path.isdir(os.path.join(ref_dir, "src", "gpu")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_dir}"], check=True)
 
 
 def lib():
@@ -96,7 +98,7 @@ def lib():
 def have_ref() -> bool:
     if os.path.exists(REF_SO):
         return True
-    if os.path.isdir(os.path.join(REF_SRC, "src", "gpu")):
+    if REF_SRC and os.path.isdir(os.path.join(REF_SRC, "src", "gpu")):
         try:
             subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
         except Exception:

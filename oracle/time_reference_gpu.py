@@ -2,7 +2,7 @@
 search_by_value with calcNCC (the NCC single-pair configuration, 256x256 float, 6^8 grid) and
 calcMIAlt (the MI configuration's images, 512x512 uint8, 5^8 grid) -- compiled unchanged for
 sm_100a in oracle/_ref, and prints one JSON line per case.  The numbers are a reported
-baseline for BASELINE.md, next to the reference's CPU path and this library's kernels.
+baseline, next to the reference's CPU path and this library's kernels.
 
 Buffers are padded as the reference's kernel needs: its result write at index n (bound check
 '>') and its bilinear taps one row past an image stay inside the allocations.

@@ -1,9 +1,9 @@
 #!/usr/bin/env python3
 """Generate the golden vectors of the grid-search parity tests from the REFERENCE itself.
 
-Run where the reference checkout exists (default /root/reference, or CGS_REFERENCE_DIR):
+Run where the reference checkout exists, naming it in CGS_REFERENCE_DIR:
 
-    python tests/golden/make_golden.py
+    CGS_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
 
 The reference has no tests and no golden vectors; its only fixtures are the 6x6 images of
 its examples (src/gpu/cudaGridSearch_example1.cu:51-71, repeated in cudaGridSearch_main.cu
@@ -32,7 +32,9 @@ sys.path.insert(0, ROOT)
 import oracle as O  # noqa: E402
 from cugridsearch_b200 import synthetic as S  # noqa: E402
 
-REF = os.environ.get("CGS_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("CGS_REFERENCE_DIR", "")
+if not REF:
+    sys.exit("set CGS_REFERENCE_DIR to the reference checkout")
 
 
 def example_images() -> dict[str, np.ndarray]:
