@@ -199,10 +199,12 @@ class CudaTensor:
 
 def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0,
              warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool | None = None,
-             quad_taps: bool | None = None) -> CgsOptions:
+             quad_taps: bool | None = None, per_sample_decisions: bool = False) -> CgsOptions:
     if cost not in COSTS:
         raise ValueError(f"unknown cost {cost!r}")
     flags = _abi.FLAG_NATURAL_ORDER if natural_order else 0
+    if per_sample_decisions:
+        flags |= _abi.FLAG_PER_SAMPLE_DECISIONS
     if quad_taps is True:
         flags |= _abi.FLAG_QUAD_TAPS
     elif quad_taps is False:
@@ -217,14 +219,16 @@ def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_
 def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs=None, stream=None,
            mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0, warps_per_block: int = 0,
            natural_order: bool = False, exact_samples: bool | None = None, result=None,
-           quad_taps: bool | None = None) -> Argmin | None:
+           quad_taps: bool | None = None, per_sample_decisions: bool = False) -> Argmin | None:
     """Run one fused search.  With ``result`` (a CUDA uint8 tensor of sizeof(cgs_argmin)
     bytes) the call is asynchronous and returns None; otherwise it synchronises and
     returns the :class:`Argmin`.  ``exact_samples``: None = the cost's default (exact for
     the reference functors, fast for ZNCC / MI), True / False force a mode.  ``quad_taps``:
-    None = the library's choice, True = pre-gathered 16-byte quads, False = texture gathers."""
+    None = the library's choice, True = pre-gathered 16-byte quads, False = texture gathers.
+    ``per_sample_decisions``: run single-channel ZNCC on the per-sample decision kernel instead of
+    the span kernel (CGS_FLAG_PER_SAMPLE_DECISIONS)."""
     opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples,
-                   quad_taps)
+                   quad_taps, per_sample_decisions)
     cptr = costs.data_ptr() if costs is not None else None
     s = _stream_handle(stream)
     L = _abi.load()

@@ -22,6 +22,7 @@ FLAG_EXACT_SAMPLES = 2
 FLAG_FAST_SAMPLES = 4
 FLAG_QUAD_TAPS = 8
 FLAG_TEXTURE_TAPS = 16
+FLAG_PER_SAMPLE_DECISIONS = 32
 
 STATUS = {
     0: "CGS_SUCCESS", 1: "CGS_ERROR_INVALID_VALUE", 2: "CGS_ERROR_UNSUPPORTED",

@@ -78,7 +78,12 @@ def _stamp(src: str, extra: list[str]) -> str:
     for f in _deps(src):
         with open(f, "rb") as fh:
             h.update(fh.read())
-    h.update(" ".join(_flags(src) + ARCH + extra).encode())
+    # flags with the checkout's own folders made relative, so a copy of the tree at another path
+    # (built objects travel with it) keeps its stamps
+    root = os.path.dirname(HERE)
+    flags = [os.path.relpath(f, root) if os.path.isabs(f) and f.startswith(root) else f
+             for f in _flags(src) + ARCH + extra]
+    h.update(" ".join(flags).encode())
     return h.hexdigest()[:16]
 
 

@@ -30,7 +30,7 @@ static const void *batch_kernel_for(const cgs_batch_plan &pl) {
 }
 
 // Scratch words of a pair (the layout the search kernels and prep_body use): argmin key,
-// task counter, status, max |moving pixel|.
+// task counter, status, max |moving pixel| (bytes 16-19), the ZNCC shifts (bytes 24-31).
 constexpr size_t kHeaderBytes = 32;
 
 // key = all ones, counter = status = 0 for n headers (a tuning run's fresh results).
@@ -368,6 +368,7 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
         p.done = reinterpret_cast<unsigned int *>(sb + 8);
         p.status = reinterpret_cast<unsigned int *>(sb + 12);
         p.vmax = reinterpret_cast<float *>(sb + 16);
+        p.shifts = reinterpret_cast<const float *>(sb + 24);
         p.mov = Plane{mstage, q.moving.height, q.moving.width, 1, pd.st.mpitch, pd.st.mplane};
         p.fix = Plane{fstage, q.fixed.height, q.fixed.width, 1, pd.st.fpitch, pd.st.fplane};
         p.costs = q.costs;

@@ -40,6 +40,7 @@ struct PrepParams {
     unsigned int *done;
     unsigned int *status;
     float *vmax;  // zeroed before the launch
+    float *shifts;       // {fixed, moving} subsample means (ZNCC shifts), written by block 0, or null
     int32_t fix_alias;   // stage the fixed image like the moving one (scanline functors)
     float *row_table;    // calcMIAlt row values, or null
     int32_t rowsf;
@@ -91,6 +92,21 @@ const void *kernel_mi(int C, int G, int NW, bool quad);
 // Scanline functors (calcSQDAlt, calcNCCAlt, calcMIAlt) and their shared-memory size.
 const void *kernel_scan(int cost, int C);
 size_t scan_smem_bytes(int cost);
+
+// Span kernel of zero-mean NCC (cgs_span.cuh): G points per warp, NW warps, tiles of 32 TX
+// columns; `check` selects the self-checking build.  And its shared-memory size.
+const void *kernel_span_zncc(int G, int NW, int TX, bool check);
+size_t span_kernel_smem(int G, int NW, int TH, int tiles, int cap);
+constexpr unsigned int kStatusSpanBounds = 0x100u;  // result status bit of the self-checking span build
+constexpr int kMinSpanCap = 1024;                   // smallest useful window stage (quads)
+struct SpanPlan {
+    int G = 4, NW = 16, TX = 2, TH = 16;
+    int tiles_x = 0, tiles_y = 0, cap = 0, pitch_mod = 0;
+    bool check = false;
+    size_t smem = 0;
+    const void *kfn = nullptr;
+};
+bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, SpanPlan *sp);
 
 // Plain-load (no texture object) variants at 4 points per warp and 16 warps, for the
 // allocation-free entry point.

@@ -58,6 +58,7 @@ struct SearchParams {
     unsigned int *done;
     unsigned int *status;
     const float *vmax;   // max |moving pixel| (from the staging kernel)
+    const float *shifts; // {fixed, moving} image means (staging kernel): the shifts of the ZNCC sums
     cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
     const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y+1, x), (y, x+1) - (y, x), (y+1, x+1) - (y+1, x)}
     int32_t quad_pitch;           // quads per row
@@ -65,6 +66,9 @@ struct SearchParams {
     const float *row_table;       // calcMIAlt's row values (the float recurrence row += 1/(H_f-1))
     int32_t n_rows;
     cgs_argmin *result;
+    // span kernel (cgs_span.cuh): rows per tile, tiles per row and column, 16-byte units per stage
+    // (the tile's fixed rows, then its window), window row pitch modulo 8
+    int32_t tile_h, tiles_x, tiles_y, win_cap, win_pitch_mod;
     // cost options
     int32_t mi_bins;
     float gate_n;        // minimum overlap terms for ZNCC / MI
@@ -192,8 +196,13 @@ template <> struct AccN<CGS_COST_NCC_REF> { static constexpr int value = 3; };
 template <> struct AccN<CGS_COST_ZNCC> { static constexpr int value = 5; };
 template <> struct AccN<CGS_COST_MI> { static constexpr int value = 1; };
 
-constexpr float kZnccShift = 127.5f;  // centre of the [0, 255] range: keeps the one-pass
-                                      // variance sums well conditioned
+// Zero-mean NCC sums one-pass moments of shifted values f' = f - s_f, m' = m - s_m, the shifts
+// being the images' means (from a fixed subsample, computed by the staging kernel); near the data
+// the moments cancel little.  FP32 partial sums per lane are reduced and accumulated in FP64, and
+// the cost is formed in FP64.  An overlap whose fixed or moving variance is below kZnccDegenerate
+// of its sum of squares around the image mean (a constant region: the variance is then below the
+// resolution of the FP32 partial sums) has no correlation: +inf.
+constexpr double kZnccDegenerate = 1e-6;
 
 // Per-pixel quantities of the fixed value, shared by the G grid points.
 struct FixTerms {
@@ -204,7 +213,7 @@ struct FixTerms {
 };
 
 template <int COST>
-__device__ __forceinline__ FixTerms fix_terms(float f, float sB, int bins) {
+__device__ __forceinline__ FixTerms fix_terms(float f, float sB, int bins, float fshift) {
     FixTerms t;
     t.f = f;
     t.a = 0.0f;
@@ -214,7 +223,7 @@ __device__ __forceinline__ FixTerms fix_terms(float f, float sB, int bins) {
         t.a = xd(f, 255.0f);
         t.b = xd(xm(t.a, f), 255.0f);
     } else if constexpr (COST == CGS_COST_ZNCC) {
-        t.a = f - kZnccShift;
+        t.a = f - fshift;
         t.b = t.a * t.a;
     } else if constexpr (COST == CGS_COST_MI) {
         t.bin = min(max((int)floorf(f * sB), 0), bins - 1);  // sB = bins / 256
@@ -222,9 +231,9 @@ __device__ __forceinline__ FixTerms fix_terms(float f, float sB, int bins) {
     return t;
 }
 
-// Accumulate one (fixed, moving value v) term.
+// Accumulate one (fixed, moving value v) term; mshift: the moving shift of ZNCC.
 template <int COST>
-__device__ __forceinline__ void accumulate(float *a, const FixTerms &t, float v) {
+__device__ __forceinline__ void accumulate(float *a, const FixTerms &t, float v, float mshift) {
     if constexpr (COST == CGS_COST_SAD_AVG || COST == CGS_COST_SAD_AVG_H || COST == CGS_COST_SAD_SUM_T ||
                   COST == CGS_COST_SAD_SUM_T_REF) {
         a[0] += fabsf(v - t.f);
@@ -242,7 +251,7 @@ __device__ __forceinline__ void accumulate(float *a, const FixTerms &t, float v)
         a[1] = fmaf(m, m, a[1]);
         a[2] += t.b;
     } else if constexpr (COST == CGS_COST_ZNCC) {
-        const float ms = v - kZnccShift;
+        const float ms = v - mshift;
         a[0] += t.a;
         a[1] += ms;
         a[2] += t.b;
@@ -262,17 +271,20 @@ __device__ __forceinline__ float finalize(const float *a, int n, const SearchPar
         return n > 0 ? xd(-a[2], sqrtf(xm(a[0], a[1]))) : 0.0f;
     } else if constexpr (COST == CGS_COST_SQD_REF) {
         return n > 0 ? xd(a[0], sqrtf(xm(a[1], a[2]))) : 123123.0f;
-    } else if constexpr (COST == CGS_COST_ZNCC) {
-        if (n == 0 || (float)n < p.gate_n) return __int_as_float(0x7f800000);
-        const float dn = (float)n;
-        const float cov = a[4] - a[0] * a[1] / dn;
-        const float vf = a[2] - a[0] * a[0] / dn;
-        const float vm = a[3] - a[1] * a[1] / dn;
-        if (!(vf > 0.0f) || !(vm > 0.0f)) return __int_as_float(0x7f800000);
-        return -cov / sqrtf(vf * vm);
     } else {
         return 0.0f;
     }
+}
+
+// Zero-mean NCC from the FP64 moments {sum f', sum m', sum f'^2, sum m'^2, sum f'm'} of n terms.
+__device__ __forceinline__ float zncc_cost(const double *a, int n, const SearchParams &p) {
+    if (n == 0 || (float)n < p.gate_n) return __int_as_float(0x7f800000);
+    const double dn = (double)n;
+    const double cov = a[4] - a[0] * a[1] / dn;
+    const double vf = a[2] - a[0] * a[0] / dn;
+    const double vm = a[3] - a[1] * a[1] / dn;
+    if (!(vf > kZnccDegenerate * a[2]) || !(vm > kZnccDegenerate * a[3])) return __int_as_float(0x7f800000);
+    return (float)(-cov / sqrt(vf * vm));
 }
 
 // ---------------------------------------------------------------- grid decode
@@ -452,6 +464,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                                          Prod &prod) {
     constexpr int NA = AccN<COST>::value;
     constexpr bool kMI = (COST == CGS_COST_MI);
+    constexpr bool kZ = (COST == CGS_COST_ZNCC);  // FP64 totals (see kZnccDegenerate)
     constexpr bool kAllPixels = (COST == CGS_COST_SAD_SUM_T_REF);  // outside samples count as 0
     constexpr bool kTexTaps = (TAPS == kTapsTexture);
     constexpr int PSTEP = BSPLIT ? NW * 32 : 32;  // pixel stride of a lane
@@ -482,6 +495,8 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
     const float gv0 = kMI ? sB * 2.0f * 8.0f * 5.9604645e-8f * (*p.vmax) + 1e-6f : 0.0f;
 
     const uint32_t ord0 = BSPLIT ? task * G : (task * NW + warp) * G;
+    const float fshift = kZ ? p.shifts[0] : 0.0f, mshift = kZ ? p.shifts[1] : 0.0f;
+    double dz[2] = {0.0, 0.0};  // ZNCC: lane l holds the warp's totals l and l + 32 of index g * NA + j
 
     FastMap fm[G];
     MiGuard mg[G];  // used by the MI instantiations only
@@ -587,7 +602,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             while (yy < rows) {
                 FixTerms ft[C];
 #pragma unroll
-                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B);
+                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B, fshift);
                 float ex[G], ey[G];
                 bool ins[G];
 #pragma unroll
@@ -632,7 +647,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                                 const int bm = min(max((int)floorf(v[g][c] * sB), 0), B - 1);
                                 atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
                             } else {
-                                accumulate<COST>(part[g], ft[c], v[g][c]);
+                                accumulate<COST>(part[g], ft[c], v[g][c], mshift);
                             }
                         }
                         cnt[g] += C;
@@ -679,7 +694,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             while (yy < rows) {
                 FixTerms ft[C];
 #pragma unroll
-                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B);
+                for (int c = 0; c < C; c++) ft[c] = fix_terms<COST>(sfix[c * R * fpitch + yy * fpitch + xx], sB, B, fshift);
                 // 1. fast coordinates, decisions and cell coordinates of all G points
                 //    (independent chains): tx = floor + 1.5 * 2^23 (round-down add), fx = floor,
                 //    ax = fraction
@@ -821,13 +836,13 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                                 const int bm = min(max((int)floorf(v[g][c] * sB), 0), B - 1);
                                 atomicAdd(&hist[g * hsize + ft[c].bin * hstride + bm], 1u);
                             } else {
-                                accumulate<COST>(part[g], ft[c], v[g][c]);
+                                accumulate<COST>(part[g], ft[c], v[g][c], mshift);
                             }
                         }
                         cnt[g] += C;
                     } else if constexpr (kAllPixels) {
 #pragma unroll
-                        for (int c = 0; c < C; c++) accumulate<COST>(part[g], ft[c], 0.0f);
+                        for (int c = 0; c < C; c++) accumulate<COST>(part[g], ft[c], 0.0f, mshift);
                         cnt[g] += C;
                     }
                 }
@@ -840,7 +855,17 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
                 }
             }
         }  // fast sampling
-        if constexpr (!kMI) {
+        if constexpr (kZ) {
+            // the chunk's warp sums into the FP64 totals
+#pragma unroll
+            for (int g = 0; g < G; g++)
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const float sw = warp_sum(part[g][j]);
+                    const int idx = g * NA + j;
+                    if (lane == (idx & 31)) dz[idx >> 5] += (double)sw;
+                }
+        } else if constexpr (!kMI) {
 #pragma unroll
             for (int g = 0; g < G; g++)
 #pragma unroll
@@ -894,6 +919,14 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             if constexpr (kMI) {
                 __syncwarp();
                 cost = mi_cost(hist + g * hsize, n);
+            } else if constexpr (kZ) {
+                double a[NA];
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int idx = g * NA + j;
+                    a[j] = __shfl_sync(0xffffffffu, dz[idx >> 5], idx & 31);
+                }
+                cost = zncc_cost(a, n, p);
             } else {
                 float a[NA];
 #pragma unroll
@@ -921,6 +954,12 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             const int n = warp_sum_i(cnt[g]);
             if (lane == 0) sm.cnts[warp * G + g] = n;
         }
+        double *dacc = reinterpret_cast<double *>(sm.acc);  // ZNCC: [NW][G * NA] FP64 totals
+        if constexpr (kZ) {
+#pragma unroll
+            for (int i = 0; i < G * NA; i++)
+                if (lane == (i & 31)) dacc[warp * G * NA + i] = dz[i >> 5];
+        }
         __syncthreads();
 #pragma unroll
         for (int g = 0; g < G; g++) {
@@ -930,6 +969,15 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
             float cost;
             if constexpr (kMI) {
                 cost = mi_cost(hist + g * hsize, n);
+            } else if constexpr (kZ) {
+                double a[NA];
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    double v = 0.0;
+                    for (int w = 0; w < NW; w++) v += dacc[w * G * NA + g * NA + j];
+                    a[j] = v;
+                }
+                cost = zncc_cost(a, n, p);
             } else {
                 float a[NA];
 #pragma unroll

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -257,13 +258,48 @@ __device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int6
     }
 }
 
-__global__ void prep_kernel(const PrepParams q) {
+// The images' means for the ZNCC shifts, over a fixed subsample (at most kShiftSamples evenly
+// strided elements of each HWC image), summed in FP64 in a fixed order by one block of 256
+// threads: the same bits on every call.  shifts = {fixed mean, moving mean}.
+constexpr int64_t kShiftSamples = 4096;
+
+__device__ void staging_means(const PrepParams &q) {
+    __shared__ double part[2][8];
+    const int t = threadIdx.x;
+    double acc[2] = {0.0, 0.0};
+    for (int k = 0; k < 2; k++) {
+        const void *src = k == 0 ? q.fix_src : q.mov_src;
+        const int pix = k == 0 ? q.fix_pix : q.mov_pix;
+        const int64_t total = k == 0 ? (int64_t)q.fh * q.fw * q.c : (int64_t)q.mh * q.mw * q.c;
+        const int64_t stride = total > kShiftSamples ? total / kShiftSamples : 1;
+        const int64_t count = total > kShiftSamples ? kShiftSamples : total;
+        double s = 0.0;
+        for (int64_t i = t; i < count; i += 256) s += (double)load_pix(src, pix, i * stride);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((t & 31) == 0) part[k][t >> 5] = s;
+        acc[k] = (double)count;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int k = 0; k < 2; k++) {
+            double s = 0.0;
+            for (int w = 0; w < 8; w++) s += part[k][w];
+            q.shifts[k] = (float)(s / acc[k]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) prep_kernel(const PrepParams q) {
+    if (blockIdx.x == 0 && q.shifts) staging_means(q);
     prep_body(q, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 // Staging of a batch: blockIdx.y selects the pair, the x blocks stride over its elements.
-__global__ void batch_prep_kernel(const PrepParams *__restrict__ qs) {
-    prep_body(qs[blockIdx.y], blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+__global__ void __launch_bounds__(256) batch_prep_kernel(const PrepParams *__restrict__ qs) {
+    const PrepParams &q = qs[blockIdx.y];
+    if (blockIdx.x == 0 && q.shifts) staging_means(q);
+    prep_body(q, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 const void *batch_prep_kernel_fn() { return (const void *)batch_prep_kernel; }
@@ -610,6 +646,7 @@ PrepParams make_prep(const cgs_image *mov, const cgs_image *fix, const Staging &
     q.done = reinterpret_cast<unsigned int *>(sb + 8);
     q.status = reinterpret_cast<unsigned int *>(sb + 12);
     q.vmax = reinterpret_cast<float *>(sb + 16);
+    q.shifts = reinterpret_cast<float *>(sb + 24);
     return q;
 }
 
@@ -643,6 +680,44 @@ static Plan choose_plan(int cost, const cgs_options &o, int mi_bins) {
     if (o.points_per_warp == 1 || o.points_per_warp == 2 || o.points_per_warp == 4) pl.G = o.points_per_warp;
     if (o.warps_per_block > 0) pl.NW = o.warps_per_block;
     return pl;
+}
+
+// Launch plan of the span kernel: points per warp (the request's 2, else 4), 16 warps, tiles of
+// 32 TX columns by TH rows (128 x 16 unless the tuning variables CGS_SPAN_TX = 1 | 2 | 4 and
+// CGS_SPAN_TH = 8 | 16 | 32 say otherwise), the window stage filling the shared memory that is
+// left (at most CGS_SPAN_CAP 16-byte units when that is set; a stage holds the tile's fixed rows
+// and its window) and window rows padded to CGS_SPAN_PITCH (mod 8) quads.  CGS_SPAN_CHECK=1 selects the self-checking build (every fast sample's quad address is
+// checked against its window; a miss sets status bit 0x100 and skips the sample).  False where
+// the span kernel does not apply: several channels, images of 32768 or more pixels a side, or
+// too many tiles for shared memory.
+static int env_int(const char *name, int dflt) {
+    const char *v = std::getenv(name);
+    return (v && *v) ? std::atoi(v) : dflt;
+}
+
+bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, SpanPlan *sp) {
+    if (fix.channels != 1 || mov.width >= 32768 || mov.height >= 32768 || fix.width >= 32768 || fix.height >= 32768)
+        return false;
+    sp->G = o.points_per_warp == 2 ? 2 : 4;
+    sp->NW = 16;
+    sp->TX = env_int("CGS_SPAN_TX", 4);
+    sp->TH = env_int("CGS_SPAN_TH", 16);
+    if (!(sp->TX == 1 || sp->TX == 2 || sp->TX == 4) || !(sp->TH == 8 || sp->TH == 16 || sp->TH == 32)) return false;
+    sp->check = env_int("CGS_SPAN_CHECK", 0) != 0;
+    sp->kfn = kernel_span_zncc(sp->G, sp->NW, sp->TX, sp->check);
+    if (!sp->kfn) return false;
+    sp->tiles_x = (fix.width + 32 * sp->TX - 1) / (32 * sp->TX);
+    sp->tiles_y = (fix.height + sp->TH - 1) / sp->TH;
+    const int tiles = sp->tiles_x * sp->tiles_y;
+    const size_t budget = 227 * 1024, fixed = span_kernel_smem(sp->G, sp->NW, sp->TH, tiles, 0);
+    if (fixed + (size_t)kMinSpanCap * 32 > budget) return false;
+    sp->cap = (int)((budget - fixed) / 32);
+    // CGS_SPAN_CAP (quads) lowers the stage size, e.g. to exercise the global-memory path
+    sp->cap = std::max(kMinSpanCap, std::min(sp->cap, env_int("CGS_SPAN_CAP", sp->cap)));
+    sp->cap = std::max(sp->cap, kMinSpanCap + sp->TH * 32 * sp->TX / 4);  // room for the fixed rows
+    sp->pitch_mod = env_int("CGS_SPAN_PITCH", 0) & 7;
+    sp->smem = span_kernel_smem(sp->G, sp->NW, sp->TH, tiles, sp->cap);
+    return sp->smem <= budget;
 }
 
 // The scanline functors: staging with both images aliased, the calcMIAlt row table, one warp
@@ -703,6 +778,7 @@ static cgs_status search_scanline(const cgs_image *mov, const cgs_image *fix, co
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
     p.vmax = reinterpret_cast<float *>(sb + 16);
+    p.shifts = reinterpret_cast<const float *>(sb + 24);
     float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
     float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
     float *rtab = mi ? reinterpret_cast<float *>(sb + st.rows_off) : nullptr;
@@ -854,7 +930,11 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     // gathers there); texture gathers (MI: scalar loads) for exact sampling and for MI
     const bool fast_path = !exact_samples(cost, o.flags) && cost != CGS_COST_MI;
     const bool quads = (o.flags & CGS_FLAG_QUAD_TAPS) || (fast_path && !(o.flags & CGS_FLAG_TEXTURE_TAPS));
-    const void *kfn = getter(C, pl.G, pl.NW, quads);
+    // zero-mean NCC on the fast path: the span kernel (row decisions, shared-memory windows)
+    SpanPlan sp;
+    const bool span = cost == CGS_COST_ZNCC && fast_path && quads && !(o.flags & CGS_FLAG_PER_SAMPLE_DECISIONS) &&
+                      span_plan(*mov, *fix, o, &sp);
+    const void *kfn = span ? sp.kfn : getter(C, pl.G, pl.NW, quads);
     if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no kernel for this channel count / tuning");
 
     DeviceInfo di;
@@ -872,8 +952,17 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     // staged layout
     const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align, false, false, quads);
     const int64_t stage_bytes = set_chunks(&p, st, C, fix->height);
-    const size_t smem = cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes, acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
+    const size_t smem = span ? sp.smem
+                             : cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes,
+                                              acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
+    if (span) {
+        p.tile_h = sp.TH;
+        p.tiles_x = sp.tiles_x;
+        p.tiles_y = sp.tiles_y;
+        p.win_cap = sp.cap;
+        p.win_pitch_mod = sp.pitch_mod;
+    }
 
     cudaMemPool_t pool;
     if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
@@ -884,6 +973,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
     p.vmax = reinterpret_cast<float *>(sb + 16);
+    p.shifts = reinterpret_cast<const float *>(sb + 24);
     float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
     float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
     p.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};
@@ -913,12 +1003,12 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
         return cuda_fail(e, "prep_kernel");
     }
 
-    const int threads = pl.NW * 32;
-    const uint32_t per_task = (uint32_t)(pl.NW * pl.G);
+    const int threads = (span ? sp.NW : pl.NW) * 32;
+    const uint32_t per_task = span ? (uint32_t)(sp.NW * sp.G) : (uint32_t)(pl.NW * pl.G);
     p.num_tasks = (p.n + per_task - 1) / per_task;
     e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                                   cudaSharedmemCarveoutMaxL1);
+    if (e == cudaSuccess && !span)
+        e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxL1);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
     if (e != cudaSuccess || per_sm < 1) {
@@ -960,6 +1050,8 @@ cgs_status cgs_search_sync(const cgs_image *mov, const cgs_image *fix, const cgs
         cudaError_t e = cudaMemcpyAsync(host_result, dres, sizeof(cgs_argmin), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) s = cuda_fail(e, "result copy");
+        else if (host_result->status & (int32_t)kStatusSpanBounds)
+            s = fail(CGS_ERROR_CUDA, "span kernel self-check: a sample's quad address left its window");
         else if (host_result->status != CGS_SUCCESS) s = fail((cgs_status)host_result->status, "device wait timed out");
     }
     cudaFreeAsync(dres, stream);
@@ -1084,6 +1176,7 @@ cgs_status cgs_search_noalloc(const cgs_image *mov, const cgs_image *fix, const 
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
     p.vmax = reinterpret_cast<float *>(sb + 16);
+    p.shifts = reinterpret_cast<const float *>(sb + 24);
     float *mstage = reinterpret_cast<float *>(sb + st.mov_off);
     float *fstage = reinterpret_cast<float *>(sb + st.fix_off);
     p.mov = Plane{mstage, mov->height, mov->width, C, st.mpitch, st.mplane};

@@ -156,7 +156,9 @@ def config2(seed: int = DEFAULT_SEED) -> Pair:
 
 def config3_pairs(seed: int = DEFAULT_SEED, n: int = 64) -> list[Pair]:
     """64 pairs, square sizes log-uniform in [128, 1024], f32; costs cycle SAD / NCC / MI;
-    translation range scaled to the size; 4-6 values per parameter."""
+    translation range scaled to the size; 4-6 values per parameter.  Images follow the NCC
+    pair's recipe scaled to the size (40 blobs, sigma 12-40 px at 256 px), so larger pairs are
+    as textured as the benchmark pair rather than saturated."""
     rng = np.random.default_rng(seed)
     pairs = []
     costs = ["SAD_AVG", "ZNCC", "MI"]
@@ -166,7 +168,7 @@ def config3_pairs(seed: int = DEFAULT_SEED, n: int = 64) -> list[Pair]:
         cost = costs[i % 3]
         lo, hi = _ranges(10, 0.1, 0.05, 24.0 * size / 256.0, 1e-4)
         kind = "uncentred" if cost == "SAD_AVG" else "centred"
-        pairs.append(make_pair(seed + 1 + i, size, max(12, size // 8), (size / 21.0, size / 6.4), lo, hi, cnt, kind,
+        pairs.append(make_pair(seed + 1 + i, size, 40, (12.0 * size / 256.0, 40.0 * size / 256.0), lo, hi, cnt, kind,
                                cost=cost))
     return pairs
 

@@ -103,6 +103,11 @@ typedef struct cgs_options {
  * only speed and scratch size differ. */
 #define CGS_FLAG_QUAD_TAPS 8
 #define CGS_FLAG_TEXTURE_TAPS 16
+/* Zero-mean NCC on the fast path runs the span kernel by default (single channel, quad taps):
+ * in/out decisions per image row, taps read from per-tile moving-image windows in shared
+ * memory.  This flag selects the per-sample decision kernel instead.  Both make the same
+ * decisions and form the same samples; costs agree within FP32 summation order. */
+#define CGS_FLAG_PER_SAMPLE_DECISIONS 32
 
 /* Argmin of a search: the lowest cost, ties broken by the lowest grid index.  NaN and
  * +inf costs never win (the reference compares with '<', cudaTensor.cuh:256 and

@@ -318,6 +318,19 @@ static inline uint32_t og_bin(float v, int bins) {
     return (uint32_t)b;
 }
 
+/* The shifts of the zero-mean NCC moments: an image's mean over a fixed subsample -- at most
+ * 4096 evenly strided elements of the HWC array (stride total / 4096), summed in double and
+ * rounded to float.  The library's staging kernel takes the same elements; a cost does not depend
+ * on its shifts beyond rounding, but the degenerate-overlap rule below is stated with them. */
+static float og_subsample_mean(const og_image *im) {
+    const int64_t total = (int64_t)im->height * im->width * im->channels;
+    const int64_t stride = total > 4096 ? total / 4096 : 1;
+    const int64_t count = total > 4096 ? 4096 : total;
+    double s = 0.0;
+    for (int64_t i = 0; i < count; i++) s += (double)og_at(im, i * stride);
+    return (float)(s / (double)count);
+}
+
 #define OG_ACC float
 #define OG_SQRT sqrtf
 #define OG_SFX _f32

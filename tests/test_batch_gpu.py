@@ -48,13 +48,15 @@ def _make(cuda, specs, seed=7):
 
 
 def _single(cuda, items):
-    """cgs_search per pair: (costs, argmin) on the host."""
+    """cgs_search per pair: (costs, argmin) on the host.  The batch runs every cost on the per-sample
+    decision kernel, so ZNCC pairs are compared with that kernel (CGS_FLAG_PER_SAMPLE_DECISIONS);
+    test_batch_zncc_agrees_with_span_kernel covers the single search's default ZNCC kernel."""
     import torch
     import cugridsearch_b200 as cgs
     out = []
     for it in items:
         c = torch.empty(it["grid"].numElements(), dtype=torch.float32, device=cuda)
-        r = cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c)
+        r = cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c, per_sample_decisions=True)
         out.append((c.cpu().numpy(), r))
     return out
 
@@ -171,7 +173,7 @@ def test_batch_graph_replay_follows_image_contents(cuda, items, reference):
             torch.cuda.synchronize()
             c_new = it["costs"].cpu().numpy()
             c_chk = torch.empty_like(it["costs"])
-            cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c_chk)
+            cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c_chk, per_sample_decisions=True)
             np.testing.assert_array_equal(c_new.view(np.uint32), c_chk.cpu().numpy().view(np.uint32))
             assert not np.array_equal(c_new, reference[1][0])
         finally:
@@ -212,3 +214,22 @@ def test_search_batched_one_shot(cuda, items, reference):
     for (c_ref, r_ref), (c, r) in zip(reference, _read(items)):
         np.testing.assert_array_equal(c.view(np.uint32), c_ref.view(np.uint32))
         assert r.index == r_ref.index
+
+
+def test_batch_zncc_agrees_with_span_kernel(cuda, items, lib):
+    """ZNCC pairs of a batch (per-sample decision kernel) against cgs_search's default ZNCC kernel
+    (the span kernel): same finite pattern, costs within the FP32 summation tolerance."""
+    import torch
+    import cugridsearch_b200 as cgs
+    with cgs.Batch(_batch_pairs(items)) as b:
+        b.launch()
+        torch.cuda.synchronize()
+    for it, (c, r) in zip(items, _read(items)):
+        if it["cost"] != "ZNCC":
+            continue
+        cs = torch.empty(it["grid"].numElements(), dtype=torch.float32, device=cuda)
+        cgs.search("ZNCC", it["mov"], it["fix"], it["grid"], costs=cs)
+        s = cs.cpu().numpy()
+        fin = np.isfinite(s)
+        np.testing.assert_array_equal(np.isfinite(c), fin)
+        assert np.max(np.abs(c[fin] - s[fin]) / np.maximum(np.abs(s[fin]), 1.0)) <= 1e-5

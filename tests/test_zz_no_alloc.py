@@ -26,18 +26,42 @@ def _run(lib, fn, mov, fix, grid, opts, costs, res, stream):
     assert status == 0, lib.cgs_last_error().decode()
 
 
-@pytest.mark.parametrize("cost,u8", [("ZNCC", False), ("MI", True), ("SAD_AVG", False)])
-def test_noalloc_matches_search_on_two_calls(cuda, lib, cost, u8):
+# Every cost the allocation-free entry point runs, single- and three-channel where the cost
+# takes several channels.  Each case's second pair has a moving image smaller than the fixed
+# one, so samples reach the moving image's last column and row (the reference's flat-index
+# neighbour at W - 1 < x < W and the zero row past the image).
+CASES = [(c, ch) for c in ("SAD_AVG", "SQD_REF", "NCC_REF", "ZNCC", "MI") for ch in (1, 3)] + \
+        [("SAD_AVG_H", 1), ("SAD_SUM_T", 1), ("SAD_SUM_T_REF", 1)]
+
+
+def _case_pairs(cost, channels):
+    u8 = cost == "MI"
+    base = "SAD_AVG" if cost in ("SAD_SUM_T", "SAD_SUM_T_REF") else cost
+    pairs = [S.small_pair(41, size=64, count=4, cost=base, u8=u8, channels=channels),
+             S.small_pair(42, size=48, count=4, cost=base, u8=u8, channels=channels, msize=37)]
+    grids = []
+    for p in pairs:
+        if cost == "SAD_AVG_H":
+            grids.append(([0.95, -0.05, -4.0, -0.05, 0.95, -4.0, -1e-4, -1e-4],
+                          [1.05, 0.05, 4.0, 0.05, 1.05, 4.0, 1e-4, 1e-4], [3] * 8))
+        elif cost in ("SAD_SUM_T", "SAD_SUM_T_REF"):
+            grids.append(([-6.0, -6.0], [6.0, 6.0], [25, 19]))
+        else:
+            grids.append(p.grid_args())
+    return pairs, grids
+
+
+@pytest.mark.parametrize("cost,channels", CASES)
+def test_noalloc_matches_search_on_two_calls(cuda, lib, cost, channels):
     import torch
     import cugridsearch_b200 as cgs
     import cugridsearch_b200._abi as abi
     stream = torch.cuda.current_stream().cuda_stream
-    pairs = [S.small_pair(41, size=64, count=4, cost=cost, u8=u8),
-             S.small_pair(42, size=48, count=4, cost=cost, u8=u8)]
-    for k, pair in enumerate(pairs):  # two calls in a row, different inputs
+    pairs, grids = _case_pairs(cost, channels)
+    for k, (pair, ga) in enumerate(zip(pairs, grids)):  # two calls in a row, different inputs
         mov = cgs.CudaImage(torch.from_numpy(pair.moving).to(cuda))
         fix = cgs.CudaImage(torch.from_numpy(pair.fixed).to(cuda))
-        grid = cgs.CudaGrid.from_ranges(*pair.grid_args())
+        grid = cgs.CudaGrid.from_ranges(*ga)
         n = grid.numElements()
         opts = abi.CgsOptions(abi.COSTS[cost], 32, 0.0, 0, 0, 0)
         ref_costs = torch.full((n,), 7e30, device=cuda)
@@ -54,6 +78,25 @@ def test_noalloc_matches_search_on_two_calls(cuda, lib, cost, u8):
         ra, rb = cgs.read_result(ref_res), cgs.read_result(na_res)
         assert rb.valid and rb.status == 0
         assert rb.index == ra.index or abs(rb.cost - ra.cost) <= REL * max(1.0, abs(ra.cost))
+
+
+@pytest.mark.parametrize("cost", ["SQD_ALT", "NCC_ALT", "MI_ALT"])
+def test_noalloc_rejects_scanline_costs(cuda, lib, cost):
+    """The scanline functors have no allocation-free kernel: the call is refused with
+    CGS_ERROR_UNSUPPORTED and a message naming the reason, and nothing runs."""
+    import torch
+    import cugridsearch_b200 as cgs
+    import cugridsearch_b200._abi as abi
+    pair = S.small_pair(44, size=32, count=3, cost=cost)
+    mov = cgs.CudaImage(torch.from_numpy(pair.moving).to(cuda))
+    fix = cgs.CudaImage(torch.from_numpy(pair.fixed).to(cuda))
+    grid = cgs.CudaGrid.from_ranges(*pair.grid_args())
+    opts = abi.CgsOptions(abi.COSTS[cost], 32, 0.0, 0, 0, 0)
+    res = cgs.result_buffer(cuda)
+    status = lib.cgs_search_noalloc(C.byref(mov.img), C.byref(fix.img), C.byref(grid.g), C.byref(opts), None,
+                                    res.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert status == 2
+    assert b"scanline" in lib.cgs_last_error()
 
 
 def test_noalloc_allocates_nothing_and_rejects_oversize(cuda, lib):
