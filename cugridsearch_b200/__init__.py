@@ -67,16 +67,26 @@ def _stream_handle(stream) -> int:
 
 @dataclass
 class Argmin:
+    """A search's result (cgs_argmin): the FP32 argmin and, from the FP64 verification pass, the
+    FP64 cost of that index, its error, the FP64 argmin among the re-scored band and the largest
+    FP32 - FP64 difference there (verified = number of points re-scored; 0: no pass ran)."""
     cost: float
     index: int
     params: np.ndarray
     valid: bool
     status: int = 0
+    verified: int = 0
+    candidates: int = 0
+    index_fp64: int = -1
+    cost_fp64: float = float("nan")
+    err_fp64: float = float("nan")
+    max_err_fp64: float = 0.0
 
     @staticmethod
     def from_struct(r: CgsArgmin) -> "Argmin":
         return Argmin(float(r.cost), int(r.index), np.array(list(r.params), dtype=np.float32), bool(r.valid),
-                      int(r.status))
+                      int(r.status), int(r.verified), int(r.candidates), int(r.index_fp64), float(r.cost_fp64),
+                      float(r.err_fp64), float(r.max_err_fp64))
 
 
 class CudaGrid:
@@ -199,10 +209,12 @@ class CudaTensor:
 
 def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0,
              warps_per_block: int = 0, natural_order: bool = False, exact_samples: bool | None = None,
-             quad_taps: bool | None = None, per_sample_decisions: bool = False) -> CgsOptions:
+             quad_taps: bool | None = None, per_sample_decisions: bool = False, verify: bool = True) -> CgsOptions:
     if cost not in COSTS:
         raise ValueError(f"unknown cost {cost!r}")
     flags = _abi.FLAG_NATURAL_ORDER if natural_order else 0
+    if not verify:
+        flags |= _abi.FLAG_NO_VERIFY
     if per_sample_decisions:
         flags |= _abi.FLAG_PER_SAMPLE_DECISIONS
     if quad_taps is True:
@@ -219,16 +231,17 @@ def _options(cost: str, mi_bins: int = 0, overlap_gate: float = 0.0, points_per_
 def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs=None, stream=None,
            mi_bins: int = 0, overlap_gate: float = 0.0, points_per_warp: int = 0, warps_per_block: int = 0,
            natural_order: bool = False, exact_samples: bool | None = None, result=None,
-           quad_taps: bool | None = None, per_sample_decisions: bool = False) -> Argmin | None:
+           quad_taps: bool | None = None, per_sample_decisions: bool = False, verify: bool = True) -> Argmin | None:
     """Run one fused search.  With ``result`` (a CUDA uint8 tensor of sizeof(cgs_argmin)
     bytes) the call is asynchronous and returns None; otherwise it synchronises and
     returns the :class:`Argmin`.  ``exact_samples``: None = the cost's default (exact for
     the reference functors, fast for ZNCC / MI), True / False force a mode.  ``quad_taps``:
     None = the library's choice, True = pre-gathered 16-byte quads, False = texture gathers.
     ``per_sample_decisions``: run single-channel ZNCC on the per-sample decision kernel instead of
-    the span kernel (CGS_FLAG_PER_SAMPLE_DECISIONS)."""
+    the span kernel (CGS_FLAG_PER_SAMPLE_DECISIONS).  ``verify``: run the FP64 verification pass
+    (the Argmin's *_fp64 fields); False sets CGS_FLAG_NO_VERIFY."""
     opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples,
-                   quad_taps, per_sample_decisions)
+                   quad_taps, per_sample_decisions, verify)
     cptr = costs.data_ptr() if costs is not None else None
     s = _stream_handle(stream)
     L = _abi.load()

@@ -23,6 +23,8 @@ FLAG_FAST_SAMPLES = 4
 FLAG_QUAD_TAPS = 8
 FLAG_TEXTURE_TAPS = 16
 FLAG_PER_SAMPLE_DECISIONS = 32
+FLAG_NO_VERIFY = 64
+VERIFY_MAX = 64
 
 STATUS = {
     0: "CGS_SUCCESS", 1: "CGS_ERROR_INVALID_VALUE", 2: "CGS_ERROR_UNSUPPORTED",
@@ -61,7 +63,9 @@ class CgsOptions(C.Structure):
 
 class CgsArgmin(C.Structure):
     _fields_ = [("cost", C.c_float), ("valid", C.c_int32), ("index", C.c_int64),
-                ("params", C.c_float * 8), ("status", C.c_int32), ("reserved", C.c_int32)]
+                ("params", C.c_float * 8), ("status", C.c_int32), ("verified", C.c_int32),
+                ("candidates", C.c_int32), ("reserved", C.c_int32), ("index_fp64", C.c_int64),
+                ("cost_fp64", C.c_double), ("err_fp64", C.c_double), ("max_err_fp64", C.c_double)]
 
 
 class CgsPair(C.Structure):

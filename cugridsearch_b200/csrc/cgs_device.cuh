@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/cugridsearch_b200.h"
+
 namespace cgs {
 
 // Explicitly rounded FP32 operations: never contracted into FMA by the compiler.  The host
@@ -180,6 +182,17 @@ __host__ __device__ __forceinline__ float key_cost(unsigned long long k) {
     memcpy(&f, &b, 4);
     return f;
 #endif
+}
+
+// The FP64 verification fields of a result before (or without) a verification pass.
+__host__ __device__ __forceinline__ void clear_verify_fields(cgs_argmin &r) {
+    r.verified = 0;
+    r.candidates = 0;
+    r.reserved = 0;
+    r.index_fp64 = -1;
+    r.cost_fp64 = __builtin_nan("");
+    r.err_fp64 = __builtin_nan("");
+    r.max_err_fp64 = 0.0;
 }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {

@@ -108,6 +108,13 @@ struct SpanPlan {
 };
 bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, SpanPlan *sp);
 
+// FP64 verification pass (cgs_verify.cu): band collection and re-scoring after a search whose
+// costs are in p.costs and result in p.result; hdr is zeroed device scratch.
+constexpr int kVerifyMax = CGS_VERIFY_MAX;
+size_t verify_scratch_bytes();
+cgs_status launch_verify(const SearchParams &p, void *hdr, cudaStream_t stream, int sms);
+bool verify_supported(int cost);
+
 // Plain-load (no texture object) variants at 4 points per warp and 16 warps, for the
 // allocation-free entry point.
 const void *kernel_sad_avg_loads(int C);

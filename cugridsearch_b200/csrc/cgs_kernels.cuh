@@ -336,7 +336,7 @@ static __device__ void write_result(const SearchParams &p) {
     const unsigned long long k = atomicAdd(p.key, 0ull);
     cgs_argmin r;
     r.status = (int32_t)atomicAdd(p.status, 0u);
-    r.reserved = 0;
+    clear_verify_fields(r);
 #pragma unroll
     for (int a = 0; a < 8; a++) r.params[a] = 0.0f;
     if (k == ~0ull) {

@@ -311,7 +311,7 @@ __global__ void empty_result_kernel(cgs_argmin *r) {
     e.index = -1;
     for (int a = 0; a < 8; a++) e.params[a] = 0.0f;
     e.status = 0;
-    e.reserved = 0;
+    clear_verify_fields(e);
     *r = e;
 }
 
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256) argmin_kernel(const float *__restrict__ v
             const unsigned long long k = atomicAdd(key, 0ull);
             cgs_argmin r;
             r.status = 0;
-            r.reserved = 0;
+            clear_verify_fields(r);
             for (int a = 0; a < 8; a++) r.params[a] = 0.0f;
             if (k == ~0ull) {
                 r.valid = 0;
@@ -980,6 +980,19 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.fix = Plane{fstage, fix->height, fix->width, C, st.fpitch, st.fplane};
     p.costs = costs;
     p.result = result;
+    // FP64 verification pass after the search: its header, and a cost dump when the caller
+    // keeps none (the pass reads the FP32 costs of the band around the minimum)
+    const bool verify = !(o.flags & CGS_FLAG_NO_VERIFY) && verify_supported(cost);
+    void *vblock = nullptr;
+    if (verify) {
+        const size_t vbytes = verify_scratch_bytes() + (costs ? 0 : (size_t)p.n * 4);
+        cudaError_t ve = cudaMallocFromPoolAsync(&vblock, vbytes, pool, stream);
+        if (ve != cudaSuccess) {
+            cudaFreeAsync(scratch, stream);
+            return cuda_fail(ve, "cudaMallocFromPoolAsync");
+        }
+        if (!costs) p.costs = reinterpret_cast<float *>(static_cast<char *>(vblock) + verify_scratch_bytes());
+    }
     if (quads) {
         p.mov_quad = reinterpret_cast<const float4 *>(sb + st.quad_off);
         p.quad_pitch = mov->width;
@@ -999,6 +1012,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {
+        if (vblock) cudaFreeAsync(vblock, stream);
         cudaFreeAsync(scratch, stream);
         return cuda_fail(e, "prep_kernel");
     }
@@ -1012,6 +1026,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
     if (e != cudaSuccess || per_sm < 1) {
+        if (vblock) cudaFreeAsync(vblock, stream);
         cudaFreeAsync(scratch, stream);
         return e != cudaSuccess ? cuda_fail(e, "search kernel setup")
                                 : fail(CGS_ERROR_UNSUPPORTED, "search kernel does not fit on an SM");
@@ -1028,6 +1043,11 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
             if (e == cudaSuccess) e = cudaEventRecord(te->last, stream);
         }
     }
+    if (s == CGS_SUCCESS && e == cudaSuccess && verify) {
+        e = cudaMemsetAsync(vblock, 0, 8, stream);  // band count and CTA ticket
+        if (e == cudaSuccess) s = launch_verify(p, vblock, stream, di.sms);
+    }
+    if (vblock) cudaFreeAsync(vblock, stream);
     cudaFreeAsync(scratch, stream);
     if (s != CGS_SUCCESS) return s;
     if (e != cudaSuccess) return cuda_fail(e, "search kernel launch");

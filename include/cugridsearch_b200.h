@@ -108,17 +108,34 @@ typedef struct cgs_options {
  * memory.  This flag selects the per-sample decision kernel instead.  Both make the same
  * decisions and form the same samples; costs agree within FP32 summation order. */
 #define CGS_FLAG_PER_SAMPLE_DECISIONS 32
+/* Skip the FP64 verification pass (see cgs_argmin).  Without the pass the verification fields
+ * read verified = 0, index_fp64 = -1, cost_fp64 = NaN. */
+#define CGS_FLAG_NO_VERIFY 64
 
 /* Argmin of a search: the lowest cost, ties broken by the lowest grid index.  NaN and
  * +inf costs never win (the reference compares with '<', cudaTensor.cuh:256 and
- * cudaTensorKernels.cuh:45-49); if no cost is finite, valid = 0 and index = -1. */
+ * cudaTensorKernels.cuh:45-49); if no cost is finite, valid = 0 and index = -1.
+ *
+ * FP64 verification (cgs_search, unless CGS_FLAG_NO_VERIFY): the search sums in FP32; afterwards
+ * every grid point whose FP32 cost lies within 2e-5 x max(1, |cost|) of the minimum (at most
+ * CGS_VERIFY_MAX of them) is re-scored on the device with the reference's exact sampling and FP64
+ * sums -- the arithmetic of an FP64 CPU oracle -- and the fields below report the result.  The
+ * band is twice the per-point FP32 tolerance, so index_fp64 is the FP64 argmin of the whole grid
+ * whenever the FP32 costs are within that tolerance. */
+#define CGS_VERIFY_MAX 64
 typedef struct cgs_argmin {
     float cost;
     int32_t valid;
     int64_t index;
-    float params[8]; /* grid point of index, decoded as CudaGrid::getGridPoint does */
-    int32_t status;  /* cgs_status of the device work (CGS_ERROR_DEVICE_TIMEOUT if a wait gave up) */
+    float params[8];      /* grid point of index, decoded as CudaGrid::getGridPoint does */
+    int32_t status;       /* cgs_status of the device work (CGS_ERROR_DEVICE_TIMEOUT if a wait gave up) */
+    int32_t verified;     /* grid points re-scored in FP64 (0: no verification pass ran) */
+    int32_t candidates;   /* grid points in the band (> verified: the first CGS_VERIFY_MAX found were re-scored) */
     int32_t reserved;
+    int64_t index_fp64;   /* lowest FP64 cost among the re-scored points, lowest index on ties (-1: none) */
+    double cost_fp64;     /* FP64 cost of `index` (NaN if not verified) */
+    double err_fp64;      /* |cost - cost_fp64| */
+    double max_err_fp64;  /* largest |FP32 cost - FP64 cost| over the re-scored points */
 } cgs_argmin;
 
 /* CudaGrid::update(changed_axis) -- updateProcess<<<1,1>>> (src/gpu/cudaGridSearch.cuh:100-105,

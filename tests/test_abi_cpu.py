@@ -135,20 +135,24 @@ def test_batch_arguments_fail_before_device_work(lib):
 
 
 def test_batch_struct_layout():
-    """The ctypes mirror of cgs_pair / cgs_batch_plan / cgs_tune_entry has the C sizes."""
+    """The ctypes mirrors of cgs_pair / cgs_batch_plan / cgs_tune_entry / cgs_argmin have the C
+    sizes and offsets."""
     import subprocess
     import tempfile
     import cugridsearch_b200._abi as abi
     src = ('#include <stdio.h>\n#include <stddef.h>\n#include "cugridsearch_b200.h"\n'
-           'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(cgs_pair), offsetof(cgs_pair, costs),'
-           ' offsetof(cgs_pair, result), sizeof(cgs_batch_plan), sizeof(cgs_tune_entry)); return 0;}\n')
+           'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(cgs_pair), offsetof(cgs_pair, costs),'
+           ' offsetof(cgs_pair, result), sizeof(cgs_batch_plan), sizeof(cgs_tune_entry), sizeof(cgs_argmin),'
+           ' offsetof(cgs_argmin, verified), offsetof(cgs_argmin, index_fp64), offsetof(cgs_argmin, max_err_fp64));'
+           ' return 0;}\n')
     with tempfile.TemporaryDirectory() as d:
         c_file, exe = os.path.join(d, "t.c"), os.path.join(d, "t")
         open(c_file, "w").write(src)
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c_file, "-o", exe], check=True)
         got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     assert got == [C.sizeof(abi.CgsPair), abi.CgsPair.costs.offset, abi.CgsPair.result.offset,
-                   C.sizeof(abi.CgsBatchPlan), C.sizeof(abi.CgsTuneEntry)]
+                   C.sizeof(abi.CgsBatchPlan), C.sizeof(abi.CgsTuneEntry), C.sizeof(abi.CgsArgmin),
+                   abi.CgsArgmin.verified.offset, abi.CgsArgmin.index_fp64.offset, abi.CgsArgmin.max_err_fp64.offset]
 
 
 def test_homography_matches_reference_host_build(lib):
