@@ -48,12 +48,34 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS["ncc"]
 METRIC = "homography evals/s"
 UNIT = "grid-point evals/s"
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one search_kernel launch on the
-# full-size workload, from a one-pass ncu capture of `bench.py --no-cpu-baseline --steps 1
-# --warmup 3` (the default ncc workload, ZNCC with the default taps): 2.05 MB read (images and
-# staging, once), 512 B written (the 6.7 MB cost dump stays in the 126 MB L2 while the kernel
-# runs).  Measured for that configuration only; the others report null.
-TRAFFIC_BYTES_PER_LAUNCH = {"ncc": 2050000 + 512}
+# DRAM bytes per launch of the dominant kernel come from an ncu capture recorded in
+# profiles/traffic.json together with a hash of the kernel sources it was taken on; the bench
+# reports the figure only while the sources still hash the same (otherwise null).
+KERNEL_SOURCES = ["cugridsearch_b200/csrc/cgs_span.cuh", "cugridsearch_b200/csrc/cgs_kernels.cuh",
+                  "cugridsearch_b200/csrc/cgs_device.cuh", "cugridsearch_b200/csrc/cgs_search.cu"]
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
+
+
+def kernel_sources_sha16() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for f in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def recorded_traffic(workload: str):
+    """(bytes per launch, provenance) of the workload's recorded capture, or (None, why)."""
+    try:
+        rec = json.load(open(TRAFFIC_FILE)).get(workload)
+    except (OSError, ValueError):
+        rec = None
+    if not rec:
+        return None, "no capture recorded for this workload"
+    if rec.get("sources_sha16") != kernel_sources_sha16():
+        return None, "the recorded capture was taken on other kernel sources"
+    return int(rec["dram_bytes"]), f"ncu capture of {rec.get('kernel')} ({rec.get('command')})"
 
 
 def max_over_ranks(x: float, world: int, device) -> float:
@@ -133,79 +155,94 @@ class ClockSampler:
         return out
 
 
-def cpu_baseline(pair, cost_ref: str, budget_s: float = 12.0):
-    """Time the reference's functor (oracle/_ref) -- or the oracle port when the reference
-    build is absent -- on a strided sample of the grid, all host threads."""
-    import oracle as O
-    kind = "reference" if O.have_ref() else "port"
-    F, M = O.Image(pair.fixed), O.Image(pair.moving)
-    g = O.make_grid(*pair.grid_args())
-    n = O.grid_num(g)
-    threads = (O.ref().cgsref_max_threads() if kind == "reference" else os.cpu_count()) or 1
+class RefSample:
+    """The reference's functor (oracle/_ref) -- or the oracle port when the reference build is
+    absent -- on a fixed strided sample of a pair's grid, on every host thread: one run of
+    run() is one timed step of the reference arm."""
 
-    def run(count, stride):
+    def __init__(self, pair, cost_ref: str, budget_s: float):
+        import oracle as O
+        self.O, self.cost = O, cost_ref
+        self.kind = "reference" if O.have_ref() else "port"
+        self.F, self.M = O.Image(pair.fixed), O.Image(pair.moving)
+        self.g = O.make_grid(*pair.grid_args())
+        self.n = O.grid_num(self.g)
+        self.threads = (O.ref().cgsref_max_threads() if self.kind == "reference" else os.cpu_count()) or 1
+        probe = max(self.threads * 2, 16)
+        per_point = self._timed(probe, self.n // probe) / probe
+        count = int(max(probe, min(self.n, budget_s / max(per_point, 1e-9))))
+        self.stride = max(1, self.n // count)
+        self.count = min(count, (self.n + self.stride - 1) // self.stride)
+
+    def _timed(self, count, stride):
         t0 = time.perf_counter()
-        if kind == "reference":
-            O.ref_search(cost_ref, g, M, F, first=0, count=count, stride=stride, threads=threads)
+        if self.kind == "reference":
+            self.O.ref_search(self.cost, self.g, self.M, self.F, first=0, count=count, stride=stride,
+                              threads=self.threads)
         else:
-            O.search(cost_ref, g, M, F, first=0, count=count, stride=stride, f64=False, threads=threads)
+            self.O.search(self.cost, self.g, self.M, self.F, first=0, count=count, stride=stride, f64=False,
+                          threads=self.threads)
         return time.perf_counter() - t0
 
-    probe = max(threads * 2, 16)
-    t = run(probe, n // probe)
-    per_point = t / probe
-    count = int(max(probe, min(n, budget_s / max(per_point, 1e-9))))
-    stride = max(1, n // count)
-    count = min(count, (n + stride - 1) // stride)
-    t = run(count, stride)
-    return {"value": count / t, "unit": UNIT, "cores": int(threads), "kind": kind,
-            "sample": f"{count} grid points of {n} (every {stride}th index), reference {cost_ref} per point, "
-                      f"{t:.1f} s on {threads} host threads; value extrapolates points/s to the full grid"}
+    def run(self) -> float:
+        """Seconds of one pass over the sample."""
+        return self._timed(self.count, self.stride)
+
+    def describe(self, seconds: float) -> str:
+        return (f"{self.count} grid points of {self.n} (every {self.stride}th index), reference {self.cost} per "
+                f"point, {seconds:.2f} s on {self.threads} host threads")
+
+
+def cpu_baseline(pair, cost_ref: str, budget_s: float = 12.0):
+    """The reported CPU baseline: points/s of the reference's functor on a bounded sample."""
+    smp = RefSample(pair, cost_ref, budget_s)
+    t = smp.run()
+    return {"value": smp.count / t, "unit": UNIT, "cores": int(smp.threads), "kind": smp.kind,
+            "sample": smp.describe(t) + "; points/s of the sample"}
 
 
 def reference_arm(args):
+    """The reference's own CPU path on the NCC pair: each step is one pass of the reference's
+    calcNCC over the same fixed strided sample of the 6^8 grid (all host threads); value =
+    sample points / step time."""
     rank, world, _ = _env_rank()
     if rank != 0:
         return 0
     from cugridsearch_b200 import synthetic as S
     pair = S.config1()
-    per_step = []
+    smp = RefSample(pair, "NCC_REF", budget_s=max(0.5, args.ref_budget))
+    times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(pair, "NCC_REF", budget_s=max(2.0, args.ref_budget))
+        t = smp.run()
         if i >= args.warmup:
-            per_step.append(r)
-    vals = [r["value"] for r in per_step]
-    v = statistics.median(vals)
-    n_points = 6 ** 8
+            times.append(t)
+    t_med = statistics.median(times)
+    v = smp.count / t_med
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_points / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_med,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "grid_points": n_points, "pixels": 65536,
+            "config": {"workload": WORKLOAD, "grid_points": smp.n, "pixels": 65536,
+                       "step": f"one pass over a fixed strided sample of {smp.count} of the {smp.n} grid points",
                        "note": "the reference has no zero-mean NCC; its calcNCC is timed on the same grid"},
-            "cpu_baseline": dict(per_step[-1], value=v),
+            "full_grid_ms_extrapolated": 1e3 * t_med * smp.n / smp.count,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": int(smp.threads), "kind": smp.kind,
+                             "sample": smp.describe(t_med)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def batch_bench(args):
-    """Batched uneven pairs: pairs/s of one persistent launch (graph replay), per-pair
-    completion latency p50/p99 from the kernel's time stamps, and the end-to-end rate with
-    the images copied in from pinned host memory and the results copied out every step."""
+def measure_batch(dev, rank: int, world: int, n_pairs: int, steps: int, warmup: int, autotune: int = 0) -> dict:
+    """The batched uneven pairs on one GPU: pairs/s of one persistent launch (graph replay, CUDA
+    events), per-pair completion latency p50/p99 from the kernel's time stamps, and the end-to-end
+    rate with the images copied in from pinned host memory and the results copied out every step."""
     import torch
     import cugridsearch_b200 as cgs
     from cugridsearch_b200 import synthetic as S
 
-    rank, world, local = _env_rank()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     t_gen = time.perf_counter()
-    pairs = S.config3_pairs(rank_seed(rank, S.DEFAULT_SEED), n=args.pairs)
+    pairs = S.config3_pairs(rank_seed(rank, S.DEFAULT_SEED), n=n_pairs)
     t_gen = time.perf_counter() - t_gen
     stream = torch.cuda.Stream(device=dev)
     host, dev_imgs, bps, results = [], [], [], []
@@ -225,19 +262,19 @@ def batch_bench(args):
     torch.cuda.synchronize(dev)
     batch = cgs.Batch(bps)
     tune = None
-    if args.autotune > 0:
+    if autotune > 0:
         t0 = time.perf_counter()
-        best, table = batch.autotune(sample_points=args.autotune)
-        tune = {"sample_points": args.autotune, "seconds": round(time.perf_counter() - t0, 2),
+        best, table = batch.autotune(sample_points=autotune)
+        tune = {"sample_points": autotune, "seconds": round(time.perf_counter() - t0, 2),
                 "best": vars(best), "table": [[vars(p), (round(ms, 3) if np.isfinite(ms) else None), st]
                                               for p, ms, st in table]}
     plan = batch.plan
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batch.launch(stream)
     stream.synchronize()
     times, lat, span = [], [], []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+    with ClockSampler(dev.index or 0) as clk:
+        for _ in range(steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -251,10 +288,9 @@ def batch_bench(args):
             span.extend(((t1.astype(np.int64) - t0.astype(np.int64)) / 1e6).tolist())
     clocks = clk.summary()
     ms = max_over_ranks(statistics.median(times), world, dev)
-    # end to end: images in from pinned host memory, the launch, results out
     res_h = [torch.empty(r.numel(), dtype=torch.uint8).pin_memory() for r in results]
     e2e = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -273,28 +309,47 @@ def batch_bench(args):
     h2d = sum(mh.numel() * mh.element_size() + fh.numel() * fh.element_size() for mh, fh in host)
     batch.close()
     e2e_ms = max_over_ranks(statistics.median(e2e), world, dev)
-    if world > 1:
-        dist.destroy_process_group()
     n = len(pairs) * world  # every rank runs its own batch (weak scaling)
-    points *= world
-    pixel_evals *= world
-    line = {"metric": "pairs/s (batched uneven pairs)", "value": n / (ms / 1e3), "unit": "pairs/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOADS["batch"], "pairs": n, "grid_points": points, "pixel_evals": pixel_evals,
-                       "plan": vars(plan), "l2": "inputs exceed L2 (staged planes + dumps of all pairs)"},
-            "grid_point_evals_per_s": points / (ms / 1e3), "pixel_evals_per_s": pixel_evals / (ms / 1e3),
+    return {"pairs": n, "ms": ms, "pairs_per_s": n / (ms / 1e3), "grid_points": points * world,
+            "pixel_evals": pixel_evals * world, "grid_point_evals_per_s": points * world / (ms / 1e3),
+            "pixel_evals_per_s": pixel_evals * world / (ms / 1e3), "plan": vars(plan),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "span_p50": float(np.percentile(span, 50)),
                            "definition": "pair finish minus the launch's first task start (globaltimer)"},
             "e2e": {"value": n / (e2e_ms / 1e3), "unit": "pairs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": sum(r.numel() for r in res_h)},
-            "gpu_launches": 2 * args.steps,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                        "samples": clocks["samples"]},
-            "status_ok": all(r.status == 0 and r.valid for r in out), "generation_s": round(t_gen, 1)}
-    if tune:
-        line["autotune"] = tune
+            "status_ok": all(r.status == 0 and r.valid for r in out), "generation_s": round(t_gen, 1),
+            "autotune": tune}
+
+
+def batch_bench(args):
+    """The batched workload as the bench line itself (--workload batch)."""
+    import torch
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    m = measure_batch(dev, rank, world, args.pairs, args.steps, args.warmup, args.autotune)
+    if world > 1:
+        dist.destroy_process_group()
+    line = {"metric": "pairs/s (batched uneven pairs)", "value": m["pairs_per_s"], "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOADS["batch"], "pairs": m["pairs"], "grid_points": m["grid_points"],
+                       "pixel_evals": m["pixel_evals"], "plan": m["plan"],
+                       "l2": "inputs exceed L2 (staged planes + dumps of all pairs)"},
+            "grid_point_evals_per_s": m["grid_point_evals_per_s"], "pixel_evals_per_s": m["pixel_evals_per_s"],
+            "latency_ms": m["latency_ms"], "e2e": m["e2e"], "gpu_launches": 2 * args.steps, "clocks": m["clocks"],
+            "status_ok": m["status_ok"], "generation_s": m["generation_s"]}
+    if m["autotune"]:
+        line["autotune"] = m["autotune"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -308,8 +363,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cost", default="ZNCC")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the same-functor (calcNCC) and batched-pairs objects of the default line")
     ap.add_argument("--points-per-warp", type=int, default=0, help="0 = library choice")
-    ap.add_argument("--ref-budget", type=float, default=6.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--ref-budget", type=float, default=2.0, help="seconds of CPU work per reference step")
     ap.add_argument("--small", action="store_true", help="3^8 grid (for profiling captures)")
     ap.add_argument("--taps", default="auto", choices=["auto", "quad", "texture"],
                     help="tap source of the fast path (auto: the library's choice)")
@@ -424,7 +481,10 @@ def main():
     h2d = mov_h.numel() * mov_h.element_size() + fix_h.numel() * fix_h.element_size()
     d2h = costs_h.numel() * 4 + res_h.numel()
 
-    # ---- roofline of the dominant kernel (search_kernel; the staging kernel is <1% of a call)
+    # ---- roofline of the dominant kernel (the search kernel; staging and the FP64 verification
+    # pass are well under 1% of a call)
+    traffic, traffic_src = (recorded_traffic(args.workload) if cost == "ZNCC" and not args.small and
+                            args.taps == "auto" else (None, "no capture recorded for this configuration"))
     flops = FLOPS_PER_PIXEL_EVAL.get(cost, 36) * n * pix
     achieved = flops / (ms_per_step / 1e3) / 1e12
     props = torch.cuda.get_device_properties(dev)
@@ -432,8 +492,8 @@ def main():
     peak = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4),
-                "traffic": (TRAFFIC_BYTES_PER_LAUNCH.get(args.workload)
-                            if cost == "ZNCC" and not args.small and args.taps == "auto" else None),
+                "traffic": traffic,
+                "traffic_source": traffic_src,
                 "peak_source": "nominal FP32 FMA rate: SMs x 128 lanes x 2 flops x max SM clock "
                                "(MEASURED_PEAKS.json holds HBM and bf16 tensor peaks only)",
                 "flops_per_pixel_eval": FLOPS_PER_PIXEL_EVAL.get(cost, 36),
@@ -449,11 +509,40 @@ def main():
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_total / args.steps},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 4 * args.steps,  # per search: staging, search, verification band, re-scoring
             "roofline": roofline,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                        "samples": clocks["samples"]},
-            "argmin": {"index": r.index, "cost": r.cost, "params": [float(x) for x in r.params]}}
+            "argmin": {"index": r.index, "cost": r.cost, "params": [float(x) for x in r.params]},
+            "fp64_verify": {"verified": r.verified, "candidates": r.candidates, "index_fp64": r.index_fp64,
+                            "argmin_agrees": bool(r.valid and r.index == r.index_fp64), "cost_fp64": r.cost_fp64,
+                            "err_fp64": r.err_fp64, "max_err_fp64": r.max_err_fp64,
+                            "definition": "grid points within 2e-5 x max(1, |best|) of the FP32 minimum re-scored "
+                                          "on the device with the reference's exact sampling and FP64 sums"}}
+    if world == 1 and args.workload == "ncc" and cost == "ZNCC" and not args.small and not args.no_extras:
+        # the reference arm's functor (calcNCC, the reference's exact sampling) on the same pair and grid
+        def step_ref():
+            cgs.search("NCC_REF", mov, fix, grid, costs=costs, result=res, stream=stream)
+        step_ref()
+        ts = []
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_ref()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        t_ref = statistics.median(ts)
+        line["same_functor"] = {"cost": "NCC_REF", "sampling": "exact (the reference's operation sequence)",
+                                "value": n / (t_ref / 1e3), "unit": UNIT, "ms_per_step": t_ref, "steps": 3,
+                                "note": "the reference arm's functor (calcNCC) on the same pair and grid"}
+        # the batched uneven pairs: one warm-up and one timed graph replay
+        line["batch"] = measure_batch(dev, rank, world, args.pairs, steps=1, warmup=1)
+        line["batch"]["workload"] = WORKLOADS["batch"]
+        line["batch"].pop("autotune", None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(pair, "NCC_REF" if cost in ("ZNCC", "NCC_REF") else cost)
