@@ -368,6 +368,10 @@ def main():
     ap.add_argument("--points-per-warp", type=int, default=0, help="0 = library choice")
     ap.add_argument("--ref-budget", type=float, default=2.0, help="seconds of CPU work per reference step")
     ap.add_argument("--small", action="store_true", help="3^8 grid (for profiling captures)")
+    ap.add_argument("--grid-counts", default=None,
+                    help="values per axis, comma-separated, in place of the workload's (profiling captures)")
+    ap.add_argument("--per-sample-decisions", action="store_true",
+                    help="ZNCC on the per-sample decision kernel instead of the span kernel")
     ap.add_argument("--taps", default="auto", choices=["auto", "quad", "texture"],
                     help="tap source of the fast path (auto: the library's choice)")
     ap.add_argument("--workload", default="ncc", choices=["ncc", "mi", "sad", "batch"],
@@ -405,6 +409,8 @@ def main():
         pair, cost = S.config1(seed), args.cost
     if args.small:
         pair.count[:] = 3
+    if args.grid_counts:
+        pair.count[:] = [float(v) for v in args.grid_counts.split(",")]
     stream = torch.cuda.Stream(device=dev)
     mov_h = torch.from_numpy(pair.moving).pin_memory()
     fix_h = torch.from_numpy(pair.fixed).pin_memory()
@@ -422,7 +428,8 @@ def main():
 
     def step():
         cgs.search(cost, mov, fix, grid, costs=costs, result=res, stream=stream, points_per_warp=args.points_per_warp,
-                   quad_taps={"auto": None, "quad": True, "texture": False}[args.taps])
+                   quad_taps={"auto": None, "quad": True, "texture": False}[args.taps],
+                   per_sample_decisions=args.per_sample_decisions)
 
     def barrier():
         if world > 1:
@@ -484,7 +491,8 @@ def main():
     # ---- roofline of the dominant kernel (the search kernel; staging and the FP64 verification
     # pass are well under 1% of a call)
     traffic, traffic_src = (recorded_traffic(args.workload) if cost == "ZNCC" and not args.small and
-                            args.taps == "auto" else (None, "no capture recorded for this configuration"))
+                            not args.grid_counts and not args.per_sample_decisions and args.taps == "auto"
+                            else (None, "no capture recorded for this configuration"))
     flops = FLOPS_PER_PIXEL_EVAL.get(cost, 36) * n * pix
     achieved = flops / (ms_per_step / 1e3) / 1e12
     props = torch.cuda.get_device_properties(dev)
@@ -503,7 +511,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blob+sinusoid generator, seed "
                                                           f"{S.DEFAULT_SEED}+rank)",
-            "config": {"workload": WORKLOADS[args.workload] + (" (3^8 grid)" if args.small else ""), "cost": cost,
+            "config": {"workload": WORKLOADS[args.workload] + (" (3^8 grid)" if args.small else "") +
+                                   (f" (grid {args.grid_counts})" if args.grid_counts else ""), "cost": cost,
                        "grid_points": n, "pixels": pix, "points_per_warp": args.points_per_warp or "tuned",
                        "taps": args.taps,
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
@@ -519,7 +528,8 @@ def main():
                             "err_fp64": r.err_fp64, "max_err_fp64": r.max_err_fp64,
                             "definition": "grid points within 2e-5 x max(1, |best|) of the FP32 minimum re-scored "
                                           "on the device with the reference's exact sampling and FP64 sums"}}
-    if world == 1 and args.workload == "ncc" and cost == "ZNCC" and not args.small and not args.no_extras:
+    reduced = args.small or bool(args.grid_counts)
+    if world == 1 and args.workload == "ncc" and cost == "ZNCC" and not reduced and not args.no_extras:
         # the reference arm's functor (calcNCC, the reference's exact sampling) on the same pair and grid
         def step_ref():
             cgs.search("NCC_REF", mov, fix, grid, costs=costs, result=res, stream=stream)
