@@ -488,6 +488,8 @@ def main():
     h2d = mov_h.numel() * mov_h.element_size() + fix_h.numel() * fix_h.element_size()
     d2h = costs_h.numel() * 4 + res_h.numel()
 
+    span_kernel = (cost == "ZNCC" and not args.per_sample_decisions and args.taps != "texture" and
+                   pair.fixed.shape[2] == 1)
     # ---- roofline of the dominant kernel (the search kernel; staging and the FP64 verification
     # pass are well under 1% of a call)
     traffic, traffic_src = (recorded_traffic(args.workload) if cost == "ZNCC" and not args.small and
@@ -518,7 +520,8 @@ def main():
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_total / args.steps},
-            "gpu_launches": 4 * args.steps,  # per search: staging, search, verification band, re-scoring
+            # per search: staging, (the span kernel's row prefix sums,) search, verification band, re-scoring
+            "gpu_launches": (5 if span_kernel else 4) * args.steps,
             "roofline": roofline,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                        "samples": clocks["samples"]},

@@ -46,6 +46,8 @@ struct PrepParams {
     int32_t rowsf;
     float4 *quad_dst;    // moving-image tap quads (W x H per channel), or null
     int64_t qplane;
+    int32_t quad_form;   // 0: {P00, P10, P01 - P00, P11 - P10}; 1 (span kernel): {P00, P01 - P00, P10 - P00,
+                         // (P11 - P10) - (P01 - P00)}, P(dy, dx) the tap at (y + dy, x + dx)
 };
 
 // Staged layout of a moving/fixed image pair inside one scratch block.
@@ -94,9 +96,14 @@ const void *kernel_scan(int cost, int C);
 size_t scan_smem_bytes(int cost);
 
 // Span kernel of zero-mean NCC (cgs_span.cuh): G points per warp, NW warps, tiles of 32 TX
-// columns; `check` selects the self-checking build.  And its shared-memory size.
+// columns; `check` selects the self-checking build.  Its shared-memory size, the largest quad
+// plane it takes, and the launch of its own staging step (the fixed rows' FP64 prefix sums, the
+// moving shift folded into the quads) after prep_kernel.
 const void *kernel_span_zncc(int G, int NW, int TX, bool check);
-size_t span_kernel_smem(int G, int NW, int TH, int tiles, int cap);
+size_t span_kernel_smem(int G, int NW, int TH, int TX, int tiles, int cap);
+int64_t span_max_quads();
+cudaError_t launch_span_prep(const float *fix, int fpitch, int fw, int fh, double2 *prefix, float4 *quads,
+                             int64_t nquads, const float *shifts, cudaStream_t stream);
 constexpr unsigned int kStatusSpanBounds = 0x100u;  // result status bit of the self-checking span build
 constexpr int kMinSpanCap = 1024;                   // smallest useful window stage (quads)
 struct SpanPlan {

@@ -61,6 +61,7 @@ struct SearchParams {
     const float *shifts; // {fixed, moving} image means (staging kernel): the shifts of the ZNCC sums
     cudaTextureObject_t mov_tex;  // the staged moving planes as one (W+1) x C(H+1) texture
     const float4 *mov_quad;       // per channel, W x H taps {(y, x), (y+1, x), (y, x+1) - (y, x), (y+1, x+1) - (y+1, x)}
+                                  // (the span kernel's form: PrepParams::quad_form 1, less the moving shift)
     int32_t quad_pitch;           // quads per row
     int64_t quad_plane;           // quads per channel
     const float *row_table;       // calcMIAlt's row values (the float recurrence row += 1/(H_f-1))
@@ -69,6 +70,7 @@ struct SearchParams {
     // span kernel (cgs_span.cuh): rows per tile, tiles per row and column, 16-byte units per stage
     // (the tile's fixed rows, then its window), window row pitch modulo 8
     int32_t tile_h, tiles_x, tiles_y, win_cap, win_pitch_mod;
+    const double2 *fix_prefix;    // span kernel: FP64 {sum f, sum f^2} prefix sums of each fixed row, W + 1 per row
     // cost options
     int32_t mi_bins;
     float gate_n;        // minimum overlap terms for ZNCC / MI

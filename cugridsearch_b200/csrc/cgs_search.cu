@@ -230,7 +230,8 @@ __device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int6
         // tap quads of the staged moving plane, the left column and the FP32 differences to the
         // right column: {P(y, x), P(y + 1, x), P(y, x + 1) - P(y, x), P(y + 1, x + 1) - P(y + 1, x)}
         // with P the padded plane (column W = the next row's pixel 0, row H = 0); the search
-        // kernel's bilinear step takes the differences as they are
+        // kernel's bilinear step takes the differences as they are.  The span kernel's form holds
+        // the bilinear polynomial's coefficients instead (quad_form 1)
         const int64_t qtot = q.qplane * q.c;
         auto P = [&](int c, int64_t y, int64_t x) -> float {
             if (y >= q.mh) return 0.0f;
@@ -242,7 +243,8 @@ __device__ __forceinline__ void prep_body(const PrepParams &q, int64_t tid, int6
             const int64_t e = i - (int64_t)c * q.qplane;
             const int64_t y = e / q.mw, x = e - y * q.mw;
             const float v00 = P(c, y, x), v10 = P(c, y + 1, x);
-            q.quad_dst[i] = make_float4(v00, v10, P(c, y, x + 1) - v00, P(c, y + 1, x + 1) - v10);
+            const float d0 = P(c, y, x + 1) - v00, d1 = P(c, y + 1, x + 1) - v10;
+            q.quad_dst[i] = q.quad_form ? make_float4(v00, d0, v10 - v00, d1 - d0) : make_float4(v00, v10, d0, d1);
         }
     }
     if (q.row_table && tid == 0) {
@@ -683,40 +685,42 @@ static Plan choose_plan(int cost, const cgs_options &o, int mi_bins) {
 }
 
 // Launch plan of the span kernel: points per warp (the request's 2, else 4), 16 warps, tiles of
-// 32 TX columns by TH rows (128 x 16 unless the tuning variables CGS_SPAN_TX = 1 | 2 | 4 and
+// 32 TX columns by TH rows (256 x 16 unless the tuning variables CGS_SPAN_TX = 2 | 4 | 8 and
 // CGS_SPAN_TH = 8 | 16 | 32 say otherwise), the window stage filling the shared memory that is
 // left (at most CGS_SPAN_CAP 16-byte units when that is set; a stage holds the tile's fixed rows
-// and its window) and window rows padded to CGS_SPAN_PITCH (mod 8) quads.  CGS_SPAN_CHECK=1 selects the self-checking build (every fast sample's quad address is
-// checked against its window; a miss sets status bit 0x100 and skips the sample).  False where
-// the span kernel does not apply: several channels, images of 32768 or more pixels a side, or
-// too many tiles for shared memory.
+// and its blocks' windows) and window rows padded to CGS_SPAN_PITCH (mod 8) quads.
+// CGS_SPAN_CHECK=1 selects the self-checking build (every fast sample's quad address is checked
+// against its window; a miss sets status bit 0x100 and skips the sample).  False where the span
+// kernel does not apply: several channels, images of 32768 or more pixels a side, moving images
+// with (W + 8) H of 2^22 or more, or too many tiles for shared memory.
 static int env_int(const char *name, int dflt) {
     const char *v = std::getenv(name);
     return (v && *v) ? std::atoi(v) : dflt;
 }
 
 bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, SpanPlan *sp) {
-    if (fix.channels != 1 || mov.width >= 32768 || mov.height >= 32768 || fix.width >= 32768 || fix.height >= 32768)
+    if (fix.channels != 1 || mov.width >= 32768 || mov.height >= 32768 || fix.width >= 32768 || fix.height >= 32768 ||
+        (int64_t)(mov.width + 8) * mov.height >= span_max_quads())
         return false;
     sp->G = o.points_per_warp == 2 ? 2 : 4;
     sp->NW = 16;
-    sp->TX = env_int("CGS_SPAN_TX", 4);
+    sp->TX = env_int("CGS_SPAN_TX", 8);
     sp->TH = env_int("CGS_SPAN_TH", 16);
-    if (!(sp->TX == 1 || sp->TX == 2 || sp->TX == 4) || !(sp->TH == 8 || sp->TH == 16 || sp->TH == 32)) return false;
+    if (!(sp->TX == 2 || sp->TX == 4 || sp->TX == 8) || !(sp->TH == 8 || sp->TH == 16 || sp->TH == 32)) return false;
     sp->check = env_int("CGS_SPAN_CHECK", 0) != 0;
     sp->kfn = kernel_span_zncc(sp->G, sp->NW, sp->TX, sp->check);
     if (!sp->kfn) return false;
     sp->tiles_x = (fix.width + 32 * sp->TX - 1) / (32 * sp->TX);
     sp->tiles_y = (fix.height + sp->TH - 1) / sp->TH;
     const int tiles = sp->tiles_x * sp->tiles_y;
-    const size_t budget = 227 * 1024, fixed = span_kernel_smem(sp->G, sp->NW, sp->TH, tiles, 0);
+    const size_t budget = 227 * 1024, fixed = span_kernel_smem(sp->G, sp->NW, sp->TH, sp->TX, tiles, 0);
     if (fixed + (size_t)kMinSpanCap * 32 > budget) return false;
     sp->cap = (int)((budget - fixed) / 32);
     // CGS_SPAN_CAP (quads) lowers the stage size, e.g. to exercise the global-memory path
     sp->cap = std::max(kMinSpanCap, std::min(sp->cap, env_int("CGS_SPAN_CAP", sp->cap)));
     sp->cap = std::max(sp->cap, kMinSpanCap + sp->TH * 32 * sp->TX / 4);  // room for the fixed rows
     sp->pitch_mod = env_int("CGS_SPAN_PITCH", 0) & 7;
-    sp->smem = span_kernel_smem(sp->G, sp->NW, sp->TH, tiles, sp->cap);
+    sp->smem = span_kernel_smem(sp->G, sp->NW, sp->TH, sp->TX, tiles, sp->cap);
     return sp->smem <= budget;
 }
 
@@ -966,9 +970,14 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
 
     cudaMemPool_t pool;
     if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
+    // the span kernel's row prefix sums follow the staging block: W_f + 1 FP64 pairs per row
+    const size_t prefix_off = (size_t)round_up((int64_t)(st.bytes - (size_t)di.tex_align), 256);
+    const size_t prefix_bytes = span ? (size_t)fix->height * (size_t)(fix->width + 1) * sizeof(double2) : 0;
     void *scratch = nullptr;
-    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes, pool, stream), "cudaMallocFromPoolAsync");
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes + (span ? prefix_bytes + 256 : 0), pool, stream),
+             "cudaMallocFromPoolAsync");
     char *sb = staging_origin(scratch, di.tex_align);
+    if (span) p.fix_prefix = reinterpret_cast<const double2 *>(sb + prefix_off);
     p.key = reinterpret_cast<unsigned long long *>(sb);
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
@@ -1003,6 +1012,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     if (quads) {
         q.quad_dst = reinterpret_cast<float4 *>(sb + st.quad_off);
         q.qplane = st.qplane;
+        q.quad_form = span ? 1 : 0;
     }
     const int64_t prep_elems = (st.mplane + st.fplane) * C;
     const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
@@ -1011,6 +1021,9 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
         prep_kernel<<<prep_blocks, 256, 0, stream>>>(q);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && span)
+        e = launch_span_prep(fstage, st.fpitch, fix->width, fix->height, const_cast<double2 *>(p.fix_prefix),
+                             reinterpret_cast<float4 *>(sb + st.quad_off), st.qplane, p.shifts, stream);
     if (e != cudaSuccess) {
         if (vblock) cudaFreeAsync(vblock, stream);
         cudaFreeAsync(scratch, stream);

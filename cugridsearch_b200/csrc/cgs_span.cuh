@@ -1,6 +1,7 @@
 // cgs_span.cuh -- the span kernel: zero-mean NCC over fast samples, with the in/out decisions
-// taken per image row instead of per sample, and the moving image's taps read from shared
-// memory.
+// taken per image row instead of per sample, the moving image's taps read from shared memory,
+// and the fixed image's sums read from row prefix sums.  Its staging step is span_prep_kernel
+// (end of this file), after the shared staging kernel has written the span form of the quads.
 //
 // Decisions per row.  For one grid point the map of a fixed row y is a projective line in the
 // moving image; the samples that lie inside the moving image form one interval of x.  Solving
@@ -10,31 +11,39 @@
 // (row, point): every pixel of the inner span is inside for the reference too and takes the
 // fast path with no test; pixels of the outer span outside the inner one (a band about a
 // thousandth of a pixel wide around the overlap's edge, almost never a whole pixel) take the
-// reference's exact operation sequence; every other pixel is outside and costs nothing.  The
-// spans are computed in FP32; their rounding error is below a quarter of the guard band (the
-// constraint terms are those the guard's own bound is built from), which the 1.5 factor covers.
+// reference's exact operation sequence, evaluated once per band of rows by the lane that
+// computed the span; every other pixel is outside and costs nothing.  The spans are computed
+// in FP32; their rounding error is below a quarter of the guard band (the constraint terms are
+// those the guard's own bound is built from), which the 1.5 factor covers.
+//
+// Fixed-image sums.  sum f and sum f^2 over a point's overlap are the inner spans' sums, taken
+// from FP64 prefix sums of each fixed row (row_prefix_kernel), plus the band pixels found
+// inside; only the three sums that involve the moving image are accumulated per sample.
 //
 // Tiles and windows.  The fixed image is walked in tiles of TW = 32 TX columns by TH rows.  For
-// every tile the CTA's grid points map the tile into a small region of the moving image (the
-// union of the tile's quadrilateral images, points of one task being neighbours in the
-// locality order); that region of the staged tap quads is copied into shared memory by bulk
-// copies, one per region row, into a two-stage mbarrier pipeline (the next tile's copies overlap
-// the current tile's sweep), and the sweep reads its 16-byte quads from there.  A region larger
-// than a stage is read from global memory instead (same values).
+// every 32-column block of a tile the CTA's grid points map the block into a small region of
+// the moving image (the union of the block's quadrilateral images, points of one task being
+// neighbours in the locality order); the regions of a tile's blocks are copied from the staged
+// tap quads into one stage of a two-stage mbarrier pipeline by bulk copies, one per region row
+// (the next tile's copies overlap the current tile's sweep), and the sweep reads its 16-byte
+// quads from there.  A block whose region does not fit the stage reads global memory instead
+// (same values).  Blocks rather than whole tiles bound the regions of rotated maps.
 //
 // Sweep.  Lane l takes the tile's columns x0 + l + 32 k; each warp evaluates its G grid points
-// at every pixel, two points per packed FP32x2 instruction.  Rows whose inner spans cover the
-// tile for every point run without any per-sample test; other rows mask samples by their spans
-// and send the band pixels down the exact path.
+// at every pixel, two points per packed FP32x2 instruction.  Blocks inside every point's inner
+// span run without any per-sample test; other blocks mask samples by the inner spans.  A
+// sample's quad index comes from the floor bits of its coordinates in one FP32x2 multiply-add
+// (x + pitch y, exact below 2^22), its address from one shift-add.
 //
-// Sums.  Per lane, per band of TH rows: five FP32 sums per point of the shifted values
-// f' = f - s_f, m' = m - s_m (the images' means; sum f', sum m', sum f'^2, sum m'^2, sum f'm'),
-// reduced across the warp at the end of each band of tiles and accumulated in FP64; the cost is
-// formed in FP64 (zncc_cost).  Which samples a lane sums, and in which order, depends only on the
-// image and the tile shape, never on the points per warp or the warps per CTA: costs are
-// bit-identical across those tunings.  The overlap count is the sum of the inner span lengths plus the band pixels
-// found inside.
+// Sums.  Per lane, per band of TH rows: three FP32 sums per point of the shifted values
+// f' = f - s_f, m' = m - s_m (the images' means; sum m', sum m'^2, sum f'm'), reduced across the
+// warp at the end of each band of tiles and accumulated in FP64 with the spans' fixed-image
+// sums and the band pixels' sums; the cost is formed in FP64 (zncc_cost).  Which samples a lane
+// sums, and in which order, depends only on the image and the tile shape, never on the points
+// per warp or the warps per CTA: costs are bit-identical across those tunings.  The overlap
+// count is the sum of the inner span lengths plus the band pixels found inside.
 #pragma once
+#include <cstddef>
 #include <type_traits>
 
 #include "cgs_kernels.cuh"
@@ -42,9 +51,12 @@
 namespace cgs {
 
 constexpr int kWinStages = 2;
+// Moving images with (W + 8) H >= 2^22 are outside the span path: the quad index x + pitch y
+// (pitch at most W + 7) is formed exactly in FP32 below that.
+constexpr int64_t kSpanMaxQuads = (int64_t)1 << 22;
 // kStatusSpanBounds (cgs_internal.h): status bit the self-checking build (CHECK = true) sets in
-// the result when a fast sample's quad address fell outside the tile's window or the quad plane
-// (the sample is then skipped).
+// the result when a fast sample's quad address fell outside its block's window or the quad
+// plane (the sample is then skipped).
 
 // Everything the span path keeps of one grid point (shared memory, one per point of the task).
 struct SpanSlot {
@@ -62,32 +74,37 @@ struct PairRow {
     float2 B, PQ, C2, RS, D2, TU;
 };
 
-// The moving-image window of one tile: quads [y0, y0 + h) x [x0, x0 + w) with row pitch `pitch`
-// quads in the stage, after the tile's fixed rows; h == 0: no point samples the tile on the fast
-// path; w < 0: the window does not fit a stage and the sweep reads global memory.
-struct TileWin {
+// The moving-image window of one 32-column block of a tile: quads [y0, y0 + h) x [x0, x0 + w)
+// with row pitch `pitch` quads, `off` quads into the stage's window area; h == 0: no point
+// samples the block on the fast path; w < 0: the window does not fit the stage and the sweep
+// reads global memory.  For the sweep: rel = 16 (off - x0 - pitch y0 - kMagicBits) (mod 2^32),
+// so that quad (ix, iy) lies at stage window + rel + 16 bits(fy pitch + tx); pitchf = pitch.
+struct BlockWin {
     int16_t x0, y0, w, h;
-    int32_t pitch, pad;
+    int32_t pitch, off;
+    uint32_t rel;
+    float pitchf;
 };
+static_assert(sizeof(BlockWin) == 24 && offsetof(BlockWin, rel) == 16, "the sweep reads {rel, pitchf} as 8 bytes");
 
-// Spans of one (point, row): inner [xa, xa + len), outer [pa, pa + plen).
-struct RowSpan {
-    int16_t xa, len, pa, plen;
+// Inner span of one (point, row): [xa, xa + len).
+struct InnerSpan {
+    int32_t xa, len;
 };
 
 // One row of a warp's points: [ia, ib] lies in every point's inner span (empty if ia > ib),
-// [ua, ub] holds every point's outer span (empty if ua > ub).
+// [ua, ub] is the hull of their inner spans (empty if ua > ub).
 struct RowRun {
     int32_t ia, ib, ua, ub;
 };
 
 __host__ __device__ constexpr size_t span_head_bytes(int NW) { return 256 + 8 * (size_t)NW; }
 
-// Shared-memory plan of the span kernel for NW warps of G points, TH-row bands, `tiles` tiles and
-// a stage of `cap` quads.
-__host__ __device__ constexpr size_t span_smem_bytes(int G, int NW, int TH, int tiles, int cap) {
+// Shared-memory plan of the span kernel for NW warps of G points, TH-row bands, tiles of TX
+// blocks, `tiles` tiles and a stage of `cap` quads.
+__host__ __device__ constexpr size_t span_smem_bytes(int G, int NW, int TH, int TX, int tiles, int cap) {
     return span_head_bytes(NW) + (size_t)NW * G * sizeof(SpanSlot) + (size_t)NW * (G / 2) * sizeof(PairRow) +
-           (size_t)tiles * sizeof(TileWin) + (size_t)NW * G * TH * sizeof(RowSpan) +
+           (size_t)tiles * TX * sizeof(BlockWin) + (size_t)NW * G * TH * sizeof(InnerSpan) +
            (size_t)NW * TH * sizeof(RowRun) + (size_t)NW * G * (5 * sizeof(double) + sizeof(int)) +
            (size_t)kWinStages * cap * 16 + 128;
 }
@@ -97,19 +114,19 @@ struct SpanSmem {
     unsigned long long *wbest;
     int *abort_flag;
     int *bounds_flag;  // self-checking build: a sample's quad address fell outside its window
-    SpanSlot *slots;  // [NW * G]
-    PairRow *prow;    // [NW * G / 2]
-    TileWin *tiles;   // [tiles]
-    RowSpan *spans;   // [NW][G][TH]
-    RowRun *runs;     // [NW][TH]
-    double *dtot;     // [NW][G * 5] FP64 task totals of the warps' points
-    int *cnt;         // [NW][G] overlap counts of the warps' points
-    float4 *win;      // [kWinStages][cap]
+    SpanSlot *slots;   // [NW * G]
+    PairRow *prow;     // [NW * G / 2]
+    BlockWin *wins;    // [tiles][TX]
+    InnerSpan *spans;  // [NW][G][TH]
+    RowRun *runs;      // [NW][TH]
+    double *dtot;      // [NW][G * 5] FP64 task totals {sum f, sum m', sum f^2, sum m'^2, sum f'm'}
+    int *cnt;          // [NW][G] overlap counts of the warps' points
+    float4 *win;       // [kWinStages][cap]
     int cap;
 };
 
 template <int G, int NW>
-__device__ __forceinline__ SpanSmem carve_span(unsigned char *smem, int TH, int tiles, int cap) {
+__device__ __forceinline__ SpanSmem carve_span(unsigned char *smem, int TH, int TX, int tiles, int cap) {
     SpanSmem s;
     s.bars = reinterpret_cast<uint64_t *>(smem);
     s.wbest = reinterpret_cast<unsigned long long *>(smem + 64);
@@ -120,10 +137,10 @@ __device__ __forceinline__ SpanSmem carve_span(unsigned char *smem, int TH, int 
     q += (size_t)NW * G * sizeof(SpanSlot);
     s.prow = reinterpret_cast<PairRow *>(q);
     q += (size_t)NW * (G / 2) * sizeof(PairRow);
-    s.tiles = reinterpret_cast<TileWin *>(q);
-    q += (size_t)tiles * sizeof(TileWin);
-    s.spans = reinterpret_cast<RowSpan *>(q);
-    q += (size_t)NW * G * TH * sizeof(RowSpan);
+    s.wins = reinterpret_cast<BlockWin *>(q);
+    q += (size_t)tiles * TX * sizeof(BlockWin);
+    s.spans = reinterpret_cast<InnerSpan *>(q);
+    q += (size_t)NW * G * TH * sizeof(InnerSpan);
     s.runs = reinterpret_cast<RowRun *>(q);
     q += (size_t)NW * TH * sizeof(RowRun);
     s.dtot = reinterpret_cast<double *>(q);
@@ -163,8 +180,8 @@ __device__ __forceinline__ void row_span(const SpanSlot &k, float yf, float s, i
     len = (none || b0 < a0) ? 0 : b0 - a0 + 1;
 }
 
-// The corners of tile [x0, x1] x [y0, y1] under a point's map: min/max of the mapped coordinates.
-__device__ __forceinline__ void tile_extent(const SpanSlot &k, float x0, float x1, float y0, float y1, float4 &e) {
+// The corners of block [x0, x1] x [y0, y1] under a point's map: min/max of the mapped coordinates.
+__device__ __forceinline__ void block_extent(const SpanSlot &k, float x0, float x1, float y0, float y1, float4 &e) {
     auto one = [&](float x, float y) {
         const float w = fmaf(k.A, x, fmaf(k.B, y, k.PQ));
         const float X = fmaf(k.C1, x, fmaf(k.C2, y, k.RS));
@@ -183,31 +200,40 @@ __device__ __forceinline__ void tile_extent(const SpanSlot &k, float x0, float x
 
 // Issue (warp 0) the copies of tile t into stage `st`, completing on that stage's barrier: the
 // tile's rows of the staged fixed image (TH x TW floats at the stage's start; columns past the
-// image's right edge are not copied) and the moving-image window (quads, after the fixed tile).
-template <int TW>
+// image's right edge are not copied) and the windows of its blocks (quads, after the fixed tile).
+template <int TX>
 __device__ __forceinline__ void issue_window(const SearchParams &p, const SpanSmem &ss, int t, int st) {
+    constexpr int TW = 32 * TX;
     const int lane = threadIdx.x & 31;
     const int TH = p.tile_h;
     const int x0 = (t % p.tiles_x) * TW, y0 = (t / p.tiles_x) * TH;
     const int rows = min(TH, p.fix.h - y0);
     const uint32_t row_bytes = (uint32_t)((min(TW, p.fix.w - x0) * 4 + 15) & ~15);  // within the row pitch
-    const TileWin tw = ss.tiles[t];
+    const BlockWin *bw = ss.wins + t * TX;
     uint64_t *bar = &ss.bars[st];
-    const bool copy = tw.h > 0 && tw.w > 0;
     if (lane == 0) {
+        uint32_t bytes = (uint32_t)rows * row_bytes;
+#pragma unroll
+        for (int c = 0; c < TX; c++)
+            if (bw[c].h > 0 && bw[c].w > 0) bytes += (uint32_t)bw[c].w * (uint32_t)bw[c].h * 16u;
         fence_proxy_async_smem();  // the stage's previous reads before the async refill
-        mbar_arrive_expect_tx(bar, (uint32_t)rows * row_bytes + (copy ? (uint32_t)tw.w * (uint32_t)tw.h * 16u : 0u));
+        mbar_arrive_expect_tx(bar, bytes);
     }
     __syncwarp();
     fence_proxy_async_smem();
     float *fdst = reinterpret_cast<float *>(ss.win + (size_t)st * ss.cap);
     for (int j = lane; j < rows; j += 32)
         bulk_g2s(fdst + j * TW, p.fix.data + (int64_t)(y0 + j) * p.fix.pitch + x0, row_bytes, bar);
-    if (copy) {
-        float4 *dst = ss.win + (size_t)st * ss.cap + TH * TW / 4;
-        const float4 *src = p.mov_quad + (int64_t)tw.y0 * p.quad_pitch + tw.x0;
-        for (int j = lane; j < tw.h; j += 32)
-            bulk_g2s(dst + (size_t)j * tw.pitch, src + (int64_t)j * p.quad_pitch, (uint32_t)tw.w * 16u, bar);
+    float4 *wdst = ss.win + (size_t)st * ss.cap + TH * TW / 4;
+#pragma unroll
+    for (int c = 0; c < TX; c++) {
+        const BlockWin b = bw[c];
+        if (b.h > 0 && b.w > 0) {
+            const float4 *src = p.mov_quad + (int64_t)b.y0 * p.quad_pitch + b.x0;
+            for (int j = lane; j < b.h; j += 32)
+                bulk_g2s(wdst + b.off + (size_t)j * b.pitch, src + (int64_t)j * p.quad_pitch, (uint32_t)b.w * 16u,
+                         bar);
+        }
     }
 }
 
@@ -227,8 +253,8 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
     const float mov_wf = p.mov_wf, mov_hf = p.mov_hf;
     const float *__restrict__ mdata = p.mov.data;
     const int mpitch = p.mov.pitch;
-    const int qpitch = p.quad_pitch;
-    const float4 *__restrict__ mquad = p.mov_quad;
+    const float *__restrict__ fdata = p.fix.data;
+    const int fpitch = p.fix.pitch;
 
     // ---- the warp's points: coefficients, guard, slots
     const uint32_t ord0 = (task * NW + warp) * G;
@@ -272,140 +298,211 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
     const float fshift = p.shifts[0], mshift = p.shifts[1];
     __syncthreads();  // every point's slot is written
 
-    // ---- windows of every tile: warp w takes tiles w, w + NW, ..; lanes take the task's points
+    // ---- windows of every block of every tile: warp w takes tiles w, w + NW, ..; lanes take the
+    // task's points
     {
         constexpr int P = NW * G;
+        const int wcap = ss.cap - TH * TW / 4;  // quads of a stage after the fixed rows
         for (int t = warp; t < ntiles; t += NW) {
             const int x0 = (t % tiles_x) * TW, y0 = (t / tiles_x) * TH;
-            const float fx0 = (float)x0, fx1 = (float)(min(x0 + TW, fw) - 1);
             const float fy0 = (float)y0, fy1 = (float)(min(y0 + TH, fh) - 1);
-            float4 e = make_float4(__int_as_float(0x7f800000), __int_as_float(0x7f800000),
+            float4 e[TX];
+#pragma unroll
+            for (int c = 0; c < TX; c++)
+                e[c] = make_float4(__int_as_float(0x7f800000), __int_as_float(0x7f800000),
                                    -__int_as_float(0x7f800000), -__int_as_float(0x7f800000));
             for (int k = lane; k < P; k += 32) {
                 const SpanSlot &sl = ss.slots[k];
-                if (sl.ok) tile_extent(sl, fx0, fx1, fy0, fy1, e);
-            }
+                if (sl.ok) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                e.x = fminf(e.x, __shfl_xor_sync(0xffffffffu, e.x, o));
-                e.y = fminf(e.y, __shfl_xor_sync(0xffffffffu, e.y, o));
-                e.z = fmaxf(e.z, __shfl_xor_sync(0xffffffffu, e.z, o));
-                e.w = fmaxf(e.w, __shfl_xor_sync(0xffffffffu, e.w, o));
-            }
-            if (lane == 0) {
-                TileWin tw{0, 0, 0, 0, 0, 0};
-                // cells a fast sample can use: floor of its coordinate (within the guard, < 1/8 px,
-                // of the real map, whose tile image lies in the corners' hull), clipped to the image
-                const float lx = fmaxf(e.x - 0.25f, -1.0f), ly = fmaxf(e.y - 0.25f, -1.0f);
-                const float hx = fminf(e.z + 0.25f, mov_wf), hy = fminf(e.w + 0.25f, mov_hf);
-                if (lx <= hx && ly <= hy) {
-                    const int cx0 = max(0, (int)floorf(lx)), cy0 = max(0, (int)floorf(ly));
-                    const int cx1 = min(p.mov.w - 1, (int)floorf(hx)), cy1 = min(p.mov.h - 1, (int)floorf(hy));
-                    if (cx0 <= cx1 && cy0 <= cy1) {
-                        const int w = cx1 - cx0 + 1, h = cy1 - cy0 + 1;
-                        const int pitch = w + ((p.win_pitch_mod - w) & 7);  // = win_pitch_mod (mod 8)
-                        tw.x0 = (int16_t)cx0;
-                        tw.y0 = (int16_t)cy0;
-                        tw.h = (int16_t)h;
-                        tw.w = (int16_t)((int64_t)pitch * h <= ss.cap - TH * TW / 4 ? w : -1);
-                        tw.pitch = pitch;
+                    for (int c = 0; c < TX; c++) {
+                        const int xc = x0 + 32 * c;
+                        if (xc < fw) block_extent(sl, (float)xc, (float)(min(xc + 32, fw) - 1), fy0, fy1, e[c]);
                     }
                 }
-                ss.tiles[t] = tw;
+            }
+#pragma unroll
+            for (int c = 0; c < TX; c++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    e[c].x = fminf(e[c].x, __shfl_xor_sync(0xffffffffu, e[c].x, o));
+                    e[c].y = fminf(e[c].y, __shfl_xor_sync(0xffffffffu, e[c].y, o));
+                    e[c].z = fmaxf(e[c].z, __shfl_xor_sync(0xffffffffu, e[c].z, o));
+                    e[c].w = fmaxf(e[c].w, __shfl_xor_sync(0xffffffffu, e[c].w, o));
+                }
+            }
+            if (lane == 0) {
+                int used = 0;
+#pragma unroll
+                for (int c = 0; c < TX; c++) {
+                    BlockWin bw{0, 0, 0, 0, 0, 0, 0u, 0.0f};
+                    // cells a fast sample can use: floor of its coordinate (within the guard, < 1/8 px,
+                    // of the real map, whose block image lies in the corners' hull), clipped to the image
+                    const float lx = fmaxf(e[c].x - 0.25f, -1.0f), ly = fmaxf(e[c].y - 0.25f, -1.0f);
+                    const float hx = fminf(e[c].z + 0.25f, mov_wf), hy = fminf(e[c].w + 0.25f, mov_hf);
+                    if (lx <= hx && ly <= hy) {
+                        const int cx0 = max(0, (int)floorf(lx)), cy0 = max(0, (int)floorf(ly));
+                        const int cx1 = min(p.mov.w - 1, (int)floorf(hx)), cy1 = min(p.mov.h - 1, (int)floorf(hy));
+                        if (cx0 <= cx1 && cy0 <= cy1) {
+                            const int w = cx1 - cx0 + 1, h = cy1 - cy0 + 1;
+                            const int pitch = w + ((p.win_pitch_mod - w) & 7);  // = win_pitch_mod (mod 8)
+                            bw.x0 = (int16_t)cx0;
+                            bw.y0 = (int16_t)cy0;
+                            bw.h = (int16_t)h;
+                            bw.pitch = pitch;
+                            if ((int64_t)pitch * h <= wcap - used) {
+                                bw.w = (int16_t)w;
+                                bw.off = used;
+                                bw.rel = 16u * ((uint32_t)used - (uint32_t)cx0 - (uint32_t)pitch * (uint32_t)cy0 -
+                                                (uint32_t)kMagicBits);
+                                bw.pitchf = (float)pitch;
+                                used += pitch * h;
+                            } else {
+                                bw.w = -1;
+                            }
+                        }
+                    }
+                    ss.wins[t * TX + c] = bw;
+                }
             }
         }
     }
     __syncthreads();
     if (warp == 0) {
-        for (int t = 0; t < kWinStages && t < ntiles; t++) issue_window<TW>(p, ss, t, (int)((wit + t) % kWinStages));
+        for (int t = 0; t < kWinStages && t < ntiles; t++) issue_window<TX>(p, ss, t, (int)((wit + t) % kWinStages));
     }
 
     // ---- sweep
-    float2 part[GP][5];
+    float2 part[GP][3];  // {sum m', sum m'^2, sum f'm'} of each pair of points
 #pragma unroll
     for (int h = 0; h < GP; h++)
 #pragma unroll
-        for (int j = 0; j < 5; j++) part[h][j] = make_float2(0.0f, 0.0f);
-    RowSpan *my_spans = ss.spans + warp * G * TH;
+        for (int j = 0; j < 3; j++) part[h][j] = make_float2(0.0f, 0.0f);
+    InnerSpan *my_spans = ss.spans + warp * G * TH;
     RowRun *my_runs = ss.runs + warp * TH;
     const float2 magic2 = make_float2(kMagic, kMagic), nmagic2 = make_float2(-kMagic, -kMagic);
     const float2 minus1 = make_float2(-1.0f, -1.0f);
-    const float2 shift2 = make_float2(-mshift, -mshift);
+    // quad index from floor bits: bits(ty + pitch fy) - kMagicBits = ix + pitch iy (exact below
+    // 2^22); global quad (ix, iy) at mqbase + 16 bits
+    const uint64_t mqbase = reinterpret_cast<uint64_t>(p.mov_quad) - 16ull * (uint64_t)(uint32_t)kMagicBits;
+    const float2 qpitch2 = make_float2((float)p.quad_pitch, (float)p.quad_pitch);
 
     for (int t = 0; t < ntiles; t++, wit++) {
         const int tx = t % tiles_x, ty = t / tiles_x;
         const int x0 = tx * TW, y0 = ty * TH;
         const int x1 = min(x0 + TW, fw) - 1;
         if (tx == 0) {
-            // spans of the band's rows, every point of the warp; inner lengths count the overlap
-            for (int i = lane; i < G * TH; i += 32) {
-                const int g = i / TH, r = i - g * TH;
-                const SpanSlot &sl = my_slots[g];
-                const int y = y0 + r;
-                RowSpan rs{0, 0, 0, 0};
-                if (y < fh && sl.valid) {
-                    if (sl.ok) {
+            // the band's rows, every point of the warp: inner spans (their fixed-image sums from the
+            // row prefix sums) and the band pixels, sampled by the reference's exact sequence;
+            // entry i = g TH + r, lanes of one point reduce over its TH rows
+            for (int k = 0; 32 * k < G * TH; k++) {
+                const int i = lane + 32 * k;
+                const bool act = i < G * TH;
+                const int g = act ? i / TH : 0, r = i - g * TH;
+                double s1 = 0.0, s2 = 0.0, sm = 0.0, smm = 0.0, sfm = 0.0;
+                int n = 0;
+                if (act) {
+                    const SpanSlot &sl = my_slots[g];
+                    const int y = y0 + r;
+                    InnerSpan is{0, 0};
+                    if (y < fh && sl.valid) {
                         const float yf = (float)y;
-                        const float wm = fmaf(sl.A, 0.5f * (float)(fw - 1), fmaf(sl.B, yf, sl.PQ));
-                        const float s = wm > 0.0f ? 1.0f : -1.0f;
-                        int xa, len, pa, plen;
-                        row_span(sl, yf, s, fw, mov_wf, mov_hf, 1.5f * sl.gx, 1.5f * sl.gy, xa, len);
-                        row_span(sl, yf, s, fw, mov_wf, mov_hf, -1.5f * sl.gx, -1.5f * sl.gy, pa, plen);
-                        if (len > 0 && plen > 0) {  // the outer span holds the inner one
-                            const int lo = min(pa, xa), hi = max(pa + plen, xa + len);
-                            pa = lo;
-                            plen = hi - lo;
-                        } else if (len > 0) {
-                            pa = xa;
-                            plen = len;
+                        int xa = 0, len = 0, pa = 0, plen = fw;  // ill-conditioned: every pixel exact
+                        if (sl.ok) {
+                            const float wm = fmaf(sl.A, 0.5f * (float)(fw - 1), fmaf(sl.B, yf, sl.PQ));
+                            const float s = wm > 0.0f ? 1.0f : -1.0f;
+                            row_span(sl, yf, s, fw, mov_wf, mov_hf, 1.5f * sl.gx, 1.5f * sl.gy, xa, len);
+                            row_span(sl, yf, s, fw, mov_wf, mov_hf, -1.5f * sl.gx, -1.5f * sl.gy, pa, plen);
+                            if (len > 0 && plen > 0) {  // the outer span holds the inner one
+                                const int lo = min(pa, xa), hi = max(pa + plen, xa + len);
+                                pa = lo;
+                                plen = hi - lo;
+                            } else if (len > 0) {
+                                pa = xa;
+                                plen = len;
+                            }
                         }
-                        rs = RowSpan{(int16_t)xa, (int16_t)len, (int16_t)pa, (int16_t)plen};
-                        if (len > 0) atomicAdd(&my_cnt[g], len);
-                    } else {
-                        rs = RowSpan{0, 0, 0, (int16_t)fw};  // ill-conditioned: every pixel exact
+                        is = InnerSpan{xa, len};
+                        if (len > 0) {
+                            const double2 *pr = p.fix_prefix + (int64_t)y * (fw + 1);
+                            const double2 a = pr[xa], b = pr[xa + len];
+                            s1 = b.x - a.x;
+                            s2 = b.y - a.y;
+                            n = len;
+                        }
+                        // band pixels: the outer span outside the inner one, [pa, e0) and [e1, pa + plen)
+                        const int e0 = len > 0 ? xa : pa + plen, e1 = len > 0 ? xa + len : pa + plen;
+                        const MapCoef kc{sl.A, sl.B, sl.P, sl.Q, sl.C1, sl.C2, sl.R, sl.S, sl.D1, sl.D2, sl.T, sl.U};
+                        const float *frow_g = fdata + (int64_t)y * fpitch;
+                        auto band = [&](int xs, int xe) {
+                            for (int x = xs; x < xe; x++) {
+                                float ex, ey;
+                                exact_map(kc, (float)x, yf, ex, ey);
+                                if (in_image(ey, ex, mov_wf, mov_hf)) {
+                                    const float m = bilinear_in(mdata, mpitch, ey, ex) - mshift;
+                                    const float f = frow_g[x];
+                                    const float fs = f - fshift;
+                                    s1 += (double)f;
+                                    s2 += (double)f * (double)f;
+                                    sm += (double)m;
+                                    smm += (double)m * (double)m;
+                                    sfm += (double)fs * (double)m;
+                                    n++;
+                                }
+                            }
+                        };
+                        band(pa, e0);
+                        band(e1, pa + plen);
                     }
+                    my_spans[g * TH + r] = is;
                 }
-                my_spans[g * TH + r] = rs;
+                // sum over the TH lanes of each point (TH is 8, 16 or 32)
+                for (int o = 1; o < TH && o < 32; o <<= 1) {
+                    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                    sm += __shfl_xor_sync(0xffffffffu, sm, o);
+                    smm += __shfl_xor_sync(0xffffffffu, smm, o);
+                    sfm += __shfl_xor_sync(0xffffffffu, sfm, o);
+                    n += __shfl_xor_sync(0xffffffffu, n, o);
+                }
+                if (act && r == 0) {
+                    double *d = my_dtot + g * 5;
+                    d[0] += s1;
+                    d[1] += sm;
+                    d[2] += s2;
+                    d[3] += smm;
+                    d[4] += sfm;
+                    my_cnt[g] += n;
+                }
             }
             __syncwarp();
-            if (lane < TH) {  // the rows' common inner run and outer hull over the warp's points
-                int ia = 0, ib = fw - 1, ua = 1 << 15, ub = -1;
+            if (lane < TH) {  // the rows' common inner run and the hull of the inner spans
+                int ia = 0, ib = fw - 1, ua = 1 << 30, ub = -1;
 #pragma unroll
                 for (int g = 0; g < G; g++) {
-                    const RowSpan rs = my_spans[g * TH + lane];
-                    if (my_slots[g].valid && rs.len > 0) {
-                        ia = max(ia, (int)rs.xa);
-                        ib = min(ib, rs.xa + rs.len - 1);
+                    const InnerSpan is = my_spans[g * TH + lane];
+                    if (is.len > 0) {
+                        ia = max(ia, is.xa);
+                        ib = min(ib, is.xa + is.len - 1);
+                        ua = min(ua, is.xa);
+                        ub = max(ub, is.xa + is.len - 1);
                     } else {
                         ib = -1;  // a point without an inner span (or outside the grid): no common run
-                    }
-                    if (rs.plen > 0) {
-                        ua = min(ua, (int)rs.pa);
-                        ub = max(ub, rs.pa + rs.plen - 1);
                     }
                 }
                 my_runs[lane] = RowRun{ia, ib, ua, ub};
             }
             __syncwarp();
         }
-        // the tile's window
+        // the tile's windows
         const int st = (int)(wit % kWinStages);
         if (!mbar_wait_bounded(&ss.bars[st], (wit / kWinStages) & 1u, kWaitLimitNs)) *ss.abort_flag = 1;
-        const TileWin tw = ss.tiles[t];
-        const bool in_smem = tw.w > 0;
-        // index of quad (ix, iy) from the bits of tx = ix + 1.5 * 2^23, ty = iy + 1.5 * 2^23: in the
-        // window, bx + pitch * by - wK = (ix - x0) + pitch * (iy - y0); in the plane, bx + qpitch *
-        // by - gK = ix + qpitch * iy (both mod 2^32, exact for in-image cells)
+        const BlockWin *twin = ss.wins + t * TX;
         const float *sfix = reinterpret_cast<const float *>(ss.win + (size_t)st * ss.cap);  // TH x TW
-        // shared address of window quad (ix, iy): sbase + 16 bx + 16 pitch by (mod 2^32)
-        const uint32_t wpitch = (uint32_t)tw.pitch;
-        const uint32_t spitch16 = 16u * wpitch;
-        const uint32_t sbase = smem_addr(ss.win + (size_t)st * ss.cap + TH * TW / 4) -
-                               16u * ((uint32_t)tw.x0 + wpitch * (uint32_t)tw.y0 + (uint32_t)kMagicBits * (1u + wpitch));
+        const uint32_t wbase = smem_addr(ss.win + (size_t)st * ss.cap + TH * TW / 4);
         const uint32_t szero = smem_addr(ss.win);
-        const uint32_t gK = (uint32_t)kMagicBits * (1u + (uint32_t)qpitch);
 
-        // one row: fast samples of G points at the lane's columns; EDGE masks by the spans
+        // one row: fast samples of G points at the lane's columns; EDGE masks by the inner spans
         auto row = [&](int r, const RowRun run) {
             const int y = y0 + r;
             const float yf = (float)y;
@@ -419,25 +516,34 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
                 byy[h] = __ffma2_rn(pr.D2, yf2, pr.TU);
             }
             const float *frow = sfix + r * TW;
-            // one block of 32 columns; EDGE: some column may lie outside a point's inner span
-            auto column = [&](int c, auto edge_tag) {
+            // one block of 32 columns; EDGE: some column may lie outside a point's inner span;
+            // SMEM: the block's window is in the stage
+            auto column = [&](int c, auto edge_tag, auto smem_tag) {
                 constexpr bool EDGE = decltype(edge_tag)::value;
-                RowSpan rsp[G];
+                constexpr bool SMEM = decltype(smem_tag)::value;
+                // shared address of window quad (ix, iy): wbase + 16 (off + (ix - x0) + pitch (iy - y0))
+                uint32_t sbase = 0u;
+                float2 pitch2 = qpitch2;
+                if constexpr (SMEM) {
+                    const uint2 rp = *reinterpret_cast<const uint2 *>(&twin[c].rel);
+                    sbase = wbase + rp.x;
+                    pitch2 = make_float2(__uint_as_float(rp.y), __uint_as_float(rp.y));
+                }
+                InnerSpan isp[G];
                 if constexpr (EDGE) {
 #pragma unroll
-                    for (int g = 0; g < G; g++) rsp[g] = my_spans[g * TH + r];
+                    for (int g = 0; g < G; g++) isp[g] = my_spans[g * TH + r];
                 }
                 const int x = x0 + 32 * c + lane;
                 const float f = frow[32 * c + lane];  // past the image's right edge: not copied, unused
                 const float fs = f - fshift;
+                const float2 fs2 = make_float2(fs, fs);
                 const float xf = (float)x;
                 const float2 xf2 = make_float2(xf, xf);
-                bool amb_any = false;
-                bool amb[G];
 #pragma unroll
                 for (int h = 0; h < GP; h++) {
                     // both points of the pair in each FP32x2 operation: map, floor (round-down add
-                    // of 1.5 * 2^23 leaves floor(m) in the mantissa), fraction
+                    // of 1.5 * 2^23 leaves floor(m) in the mantissa), fraction, quad index
                     const float2 w = __ffma2_rn(A2[h], xf2, byw[h]);
                     const float2 X = __ffma2_rn(C12[h], xf2, byx[h]);
                     const float2 Y = __ffma2_rn(D12[h], xf2, byy[h]);
@@ -446,122 +552,94 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
                     const float2 tx2 = __fadd2_rd(mx, magic2), ty2 = __fadd2_rd(my, magic2);
                     const float2 fx2 = __fadd2_rn(tx2, nmagic2), fy2 = __fadd2_rn(ty2, nmagic2);
                     const float2 ax2 = __ffma2_rn(fx2, minus1, mx), ay2 = __ffma2_rn(fy2, minus1, my);
-                    const float2 axy0 = make_float2(ax2.x, ay2.x), axy1 = make_float2(ax2.y, ay2.y);
-                    const float2 txy0 = make_float2(tx2.x, ty2.x), txy1 = make_float2(tx2.y, ty2.y);
+                    const float2 qi = __ffma2_rn(fy2, pitch2, tx2);
                     bool in0 = true, in1 = true;
                     if constexpr (EDGE) {
-                        const RowSpan a = rsp[2 * h], b = rsp[2 * h + 1];
+                        const InnerSpan a = isp[2 * h], b = isp[2 * h + 1];
                         in0 = (unsigned)(x - a.xa) < (unsigned)a.len;
                         in1 = (unsigned)(x - b.xa) < (unsigned)b.len;
-                        amb[2 * h] = !in0 && (unsigned)(x - a.pa) < (unsigned)a.plen;
-                        amb[2 * h + 1] = !in1 && (unsigned)(x - b.pa) < (unsigned)b.plen;
-                        amb_any |= amb[2 * h] | amb[2 * h + 1];
                     }
-                    float v0, v1;
-                    {
-                        const uint32_t bx0 = __float_as_uint(txy0.x), by0 = __float_as_uint(txy0.y);
-                        const uint32_t bx1 = __float_as_uint(txy1.x), by1 = __float_as_uint(txy1.y);
-                        float4 q0, q1;
-                        if (in_smem) {
-                            uint32_t a0 = sbase + by0 * spitch16 + bx0 * 16u;
-                            uint32_t a1 = sbase + by1 * spitch16 + bx1 * 16u;
-                            if constexpr (EDGE) {
-                                a0 = in0 ? a0 : szero;
-                                a1 = in1 ? a1 : szero;
-                            }
-                            if constexpr (CHECK) {  // inside the tile's window, else recorded and skipped
-                                const bool b0 = in0 && ((unsigned)((int)(bx0 - (uint32_t)kMagicBits) - tw.x0) >= (unsigned)tw.w ||
-                                                        (unsigned)((int)(by0 - (uint32_t)kMagicBits) - tw.y0) >= (unsigned)tw.h);
-                                const bool b1 = in1 && ((unsigned)((int)(bx1 - (uint32_t)kMagicBits) - tw.x0) >= (unsigned)tw.w ||
-                                                        (unsigned)((int)(by1 - (uint32_t)kMagicBits) - tw.y0) >= (unsigned)tw.h);
-                                if (b0 | b1) *ss.bounds_flag = 1;
-                                a0 = b0 ? szero : a0;
-                                a1 = b1 ? szero : a1;
-                            }
-                            // the stage is ready (its barrier was waited on above); volatile keeps the
-                            // loads after that wait
-                            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                                         : "=f"(q0.x), "=f"(q0.y), "=f"(q0.z), "=f"(q0.w) : "r"(a0));
-                            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                                         : "=f"(q1.x), "=f"(q1.y), "=f"(q1.z), "=f"(q1.w) : "r"(a1));
-                        } else {
-                            uint32_t o0 = bx0 + by0 * (uint32_t)qpitch - gK;
-                            uint32_t o1 = bx1 + by1 * (uint32_t)qpitch - gK;
-                            if constexpr (EDGE) {
-                                o0 = in0 ? o0 : 0u;
-                                o1 = in1 ? o1 : 0u;
-                            }
-                            if constexpr (CHECK) {  // inside the moving image, else recorded and skipped
-                                const bool b0 = (unsigned)((int)(bx0 - (uint32_t)kMagicBits)) >= (unsigned)p.mov.w ||
-                                                (unsigned)((int)(by0 - (uint32_t)kMagicBits)) >= (unsigned)p.mov.h;
-                                const bool b1 = (unsigned)((int)(bx1 - (uint32_t)kMagicBits)) >= (unsigned)p.mov.w ||
-                                                (unsigned)((int)(by1 - (uint32_t)kMagicBits)) >= (unsigned)p.mov.h;
-                                if ((in0 && b0) | (in1 && b1)) *ss.bounds_flag = 1;
-                                o0 = (in0 && b0) ? 0u : o0;
-                                o1 = (in1 && b1) ? 0u : o1;
-                            }
-                            q0 = __ldg(mquad + o0);
-                            q1 = __ldg(mquad + o1);
-                        }
-                        // quad = {left column, its differences to the right column}: the row lerps
-                        const float t0 = fmaf(axy0.x, q0.z, q0.x), b0 = fmaf(axy0.x, q0.w, q0.y);
-                        const float t1 = fmaf(axy1.x, q1.z, q1.x), b1 = fmaf(axy1.x, q1.w, q1.y);
-                        v0 = fmaf(axy0.y, b0 - t0, t0);
-                        v1 = fmaf(axy1.y, b1 - t1, t1);
-                    }
-                    float2 ms = __fadd2_rn(make_float2(v0, v1), shift2);
-                    float2 fm2 = make_float2(fs, fs);
+                    uint32_t q0b = __float_as_uint(qi.x), q1b = __float_as_uint(qi.y);
                     if constexpr (EDGE) {
-                        ms = make_float2(in0 ? ms.x : 0.0f, in1 ? ms.y : 0.0f);
-                        fm2 = make_float2(in0 ? fs : 0.0f, in1 ? fs : 0.0f);
+                        q0b = in0 ? q0b : (uint32_t)kMagicBits;
+                        q1b = in1 ? q1b : (uint32_t)kMagicBits;
                     }
-                    part[h][0] = __fadd2_rn(part[h][0], fm2);
-                    part[h][1] = __fadd2_rn(part[h][1], ms);
-                    part[h][2] = __ffma2_rn(fm2, fm2, part[h][2]);
-                    part[h][3] = __ffma2_rn(ms, ms, part[h][3]);
-                    part[h][4] = __ffma2_rn(fm2, ms, part[h][4]);
-                }
-                if constexpr (EDGE) {
-                    // band pixels: the reference's exact operation sequence decides and samples
-                    if (__any_sync(0xffffffffu, amb_any)) {
-#pragma unroll
-                        for (int g = 0; g < G; g++) {
-                            if (amb[g]) {
-                                const SpanSlot &sl = my_slots[g];
-                                const MapCoef kc{sl.A, sl.B, sl.P, sl.Q, sl.C1, sl.C2, sl.R, sl.S,
-                                                 sl.D1, sl.D2, sl.T, sl.U};
-                                float ex, ey;
-                                exact_map(kc, xf, yf, ex, ey);
-                                if (in_image(ey, ex, mov_wf, mov_hf)) {
-                                    const float m = bilinear_in(mdata, mpitch, ey, ex) - mshift;
-                                    if (g & 1) {
-                                        part[g / 2][0].y += fs;
-                                        part[g / 2][1].y += m;
-                                        part[g / 2][2].y = fmaf(fs, fs, part[g / 2][2].y);
-                                        part[g / 2][3].y = fmaf(m, m, part[g / 2][3].y);
-                                        part[g / 2][4].y = fmaf(fs, m, part[g / 2][4].y);
-                                    } else {
-                                        part[g / 2][0].x += fs;
-                                        part[g / 2][1].x += m;
-                                        part[g / 2][2].x = fmaf(fs, fs, part[g / 2][2].x);
-                                        part[g / 2][3].x = fmaf(m, m, part[g / 2][3].x);
-                                        part[g / 2][4].x = fmaf(fs, m, part[g / 2][4].x);
-                                    }
-                                    atomicAdd(&my_cnt[g], 1);
-                                }
-                            }
+                    float4 q0, q1;
+                    if constexpr (SMEM) {
+                        uint32_t a0 = sbase + (q0b << 4), a1 = sbase + (q1b << 4);
+                        if constexpr (EDGE) {
+                            a0 = in0 ? a0 : szero;
+                            a1 = in1 ? a1 : szero;
                         }
+                        if constexpr (CHECK) {  // inside the block's window, else recorded and skipped
+                            const BlockWin bw = twin[c];
+                            const int ix0 = (int)(__float_as_uint(tx2.x) - (uint32_t)kMagicBits) - bw.x0;
+                            const int iy0 = (int)(__float_as_uint(ty2.x) - (uint32_t)kMagicBits) - bw.y0;
+                            const int ix1 = (int)(__float_as_uint(tx2.y) - (uint32_t)kMagicBits) - bw.x0;
+                            const int iy1 = (int)(__float_as_uint(ty2.y) - (uint32_t)kMagicBits) - bw.y0;
+                            const bool b0 = in0 && ((unsigned)ix0 >= (unsigned)bw.w || (unsigned)iy0 >= (unsigned)bw.h);
+                            const bool b1 = in1 && ((unsigned)ix1 >= (unsigned)bw.w || (unsigned)iy1 >= (unsigned)bw.h);
+                            if (b0 | b1) *ss.bounds_flag = 1;
+                            a0 = b0 ? szero : a0;
+                            a1 = b1 ? szero : a1;
+                        }
+                        // the stage is ready (its barrier was waited on above); volatile keeps the
+                        // loads after that wait
+                        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                                     : "=f"(q0.x), "=f"(q0.y), "=f"(q0.z), "=f"(q0.w) : "r"(a0));
+                        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                                     : "=f"(q1.x), "=f"(q1.y), "=f"(q1.z), "=f"(q1.w) : "r"(a1));
+                    } else {
+                        if constexpr (CHECK) {  // inside the moving image, else recorded and skipped
+                            const int ix0 = (int)(__float_as_uint(tx2.x) - (uint32_t)kMagicBits);
+                            const int iy0 = (int)(__float_as_uint(ty2.x) - (uint32_t)kMagicBits);
+                            const int ix1 = (int)(__float_as_uint(tx2.y) - (uint32_t)kMagicBits);
+                            const int iy1 = (int)(__float_as_uint(ty2.y) - (uint32_t)kMagicBits);
+                            const bool b0 = in0 && ((unsigned)ix0 >= (unsigned)p.mov.w || (unsigned)iy0 >= (unsigned)p.mov.h);
+                            const bool b1 = in1 && ((unsigned)ix1 >= (unsigned)p.mov.w || (unsigned)iy1 >= (unsigned)p.mov.h);
+                            if (b0 | b1) *ss.bounds_flag = 1;
+                            q0b = b0 ? (uint32_t)kMagicBits : q0b;
+                            q1b = b1 ? (uint32_t)kMagicBits : q1b;
+                        }
+                        q0 = __ldg(reinterpret_cast<const float4 *>(mqbase + 16ull * q0b));
+                        q1 = __ldg(reinterpret_cast<const float4 *>(mqbase + 16ull * q1b));
                     }
+                    // quad = the bilinear polynomial's coefficients {c00 - s_m, c10, c01, c11}:
+                    // m' = (c00 - s_m + ax c10) + ay (c01 + ax c11)
+                    const float u0 = fmaf(ax2.x, q0.y, q0.x), w0 = fmaf(ax2.x, q0.w, q0.z);
+                    const float u1 = fmaf(ax2.y, q1.y, q1.x), w1 = fmaf(ax2.y, q1.w, q1.z);
+                    float2 ms = make_float2(fmaf(ay2.x, w0, u0), fmaf(ay2.y, w1, u1));
+                    float2 fm = fs2;
+                    if constexpr (EDGE) {  // by selection: a NaN outside the overlap stays out of the sums
+                        ms = make_float2(in0 ? ms.x : 0.0f, in1 ? ms.y : 0.0f);
+                        fm = make_float2(in0 ? fs : 0.0f, in1 ? fs : 0.0f);
+                    }
+                    part[h][0] = __fadd2_rn(part[h][0], ms);
+                    part[h][1] = __ffma2_rn(ms, ms, part[h][1]);
+                    part[h][2] = __ffma2_rn(fm, ms, part[h][2]);
                 }
             };
-            // blocks of 32 columns inside every point's inner span run unmasked
-#pragma unroll 1
-            for (int c = 0; c < TX; c++) {
-                const int xc = x0 + 32 * c;
-                if (xc > run.ub || xc + 31 < run.ua) continue;  // no point samples these columns
-                if (xc >= run.ia && xc + 31 <= run.ib) column(c, std::false_type{});
-                else column(c, std::true_type{});
+            auto block = [&](int c, auto edge_tag) {
+                if (twin[c].w > 0) column(c, edge_tag, std::true_type{});
+                else column(c, edge_tag, std::false_type{});
+            };
+            // blocks with any inner span: [cu0, cu1]; those inside every point's inner span,
+            // [cf0, cf1], run unmasked
+            const int cu0 = max(0, (run.ua - x0) >> 5), cu1 = min(TX - 1, (run.ub - x0) >> 5);
+            int cf0 = cu1 + 1, cf1 = cu1;
+            if (run.ia <= run.ib) {
+                const int a = max(cu0, (run.ia - x0 + 31) >> 5), b = min(cu1, ((run.ib - x0 + 1) >> 5) - 1);
+                if (a <= b) {
+                    cf0 = a;
+                    cf1 = b;
+                }
             }
+#pragma unroll 1
+            for (int c = cu0; c < cf0; c++) block(c, std::true_type{});
+#pragma unroll 1
+            for (int c = cf0; c <= cf1; c++) block(c, std::false_type{});
+#pragma unroll 1
+            for (int c = cf1 + 1; c <= cu1; c++) block(c, std::true_type{});
         };
         for (int r = 0; r < TH; r++) {
             if (y0 + r >= fh) break;
@@ -574,12 +652,12 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
 #pragma unroll
             for (int h = 0; h < GP; h++)
 #pragma unroll
-                for (int j = 0; j < 5; j++) {
+                for (int j = 0; j < 3; j++) {
+                    const int slot = j == 0 ? 1 : (j == 1 ? 3 : 4);  // sum m', sum m'^2, sum f'm'
                     const float s0 = warp_sum(part[h][j].x), s1 = warp_sum(part[h][j].y);
-                    const int i0 = (2 * h) * 5 + j, i1 = (2 * h + 1) * 5 + j;
                     if (lane == 0) {
-                        my_dtot[i0] += (double)s0;
-                        my_dtot[i1] += (double)s1;
+                        my_dtot[(2 * h) * 5 + slot] += (double)s0;
+                        my_dtot[(2 * h + 1) * 5 + slot] += (double)s1;
                     }
                     part[h][j] = make_float2(0.0f, 0.0f);
                 }
@@ -595,7 +673,7 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
             }
             return false;
         }
-        if (warp == 0 && t + kWinStages < ntiles) issue_window<TW>(p, ss, t + kWinStages, st);
+        if (warp == 0 && t + kWinStages < ntiles) issue_window<TX>(p, ss, t + kWinStages, st);
     }
 
     // ---- per grid point: finalise, dump, argmin key (as the pixel-loop kernel)
@@ -603,10 +681,17 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
     unsigned long long kk = ~0ull;
     if (lane < G) {
         const SpanSlot &sl = my_slots[lane];
+        const int n = my_cnt[lane];
+        // the fixed-image sums were taken unshifted: sum f' = sum f - n s, sum f'^2 = sum f^2 -
+        // 2 s sum f + n s^2 (FP64)
+        const double s = (double)fshift, dn = (double)n;
         double a[5];
 #pragma unroll
         for (int j = 0; j < 5; j++) a[j] = my_dtot[lane * 5 + j];
-        const float cost = zncc_cost(a, my_cnt[lane], p);
+        const double f1 = a[0];
+        a[0] = f1 - dn * s;
+        a[2] = a[2] - 2.0 * s * f1 + dn * s * s;
+        const float cost = zncc_cost(a, n, p);
         if (sl.valid) {
             if (p.costs) p.costs[sl.index] = cost;
             kk = make_key(cost, sl.index);
@@ -628,7 +713,7 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
 template <int G, int NW, int TX, bool CHECK>
 __global__ void __launch_bounds__(NW * 32, 1) span_kernel(const __grid_constant__ SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const SpanSmem ss = carve_span<G, NW>(smem, p.tile_h, p.tiles_x * p.tiles_y, p.win_cap);
+    const SpanSmem ss = carve_span<G, NW>(smem, p.tile_h, TX, p.tiles_x * p.tiles_y, p.win_cap);
     if (threadIdx.x == 0) {
         for (int s = 0; s < kWinStages; s++) mbar_init(&ss.bars[s], 1);
         fence_mbar_init();
@@ -644,6 +729,46 @@ __global__ void __launch_bounds__(NW * 32, 1) span_kernel(const __grid_constant_
             if (threadIdx.x == 0) retire_tasks(p, ~0ull, my_tasks - k, true);
             return;
         }
+    }
+}
+
+// The span kernel's staging step, after prep_kernel: blocks [0, row_blocks) write the FP64
+// prefix sums of each staged fixed row, prefix[y (W + 1) + x] = {sum f, sum f^2} of pixels
+// 0 .. x - 1 of row y (channel 0; one warp per row, a warp scan per 32 pixels carried in order,
+// so the sums are the same in every run); the other blocks subtract the moving image's shift
+// from every quad's constant term, so that the sweep's bilinear values are shifted already.
+__global__ void __launch_bounds__(256) span_prep_kernel(const float *__restrict__ fix, int fpitch, int fw, int fh,
+                                                        double2 *__restrict__ prefix, int row_blocks,
+                                                        float4 *__restrict__ quads, int64_t nquads,
+                                                        const float *__restrict__ shifts) {
+    if ((int)blockIdx.x >= row_blocks) {
+        const float ms = shifts[1];
+        const int64_t nthr = (int64_t)(gridDim.x - row_blocks) * blockDim.x;
+        for (int64_t i = (int64_t)(blockIdx.x - row_blocks) * blockDim.x + threadIdx.x; i < nquads; i += nthr)
+            quads[i].x -= ms;
+        return;
+    }
+    const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (row >= fh) return;
+    const float *src = fix + (int64_t)row * fpitch;
+    double2 *dst = prefix + (int64_t)row * (fw + 1);
+    if (lane == 0) dst[0] = make_double2(0.0, 0.0);
+    double c1 = 0.0, c2 = 0.0;
+    for (int x0 = 0; x0 < fw; x0 += 32) {
+        const int x = x0 + lane;
+        double v = x < fw ? (double)src[x] : 0.0;
+        double v2 = v * v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double t1 = __shfl_up_sync(0xffffffffu, v, o), t2 = __shfl_up_sync(0xffffffffu, v2, o);
+            if (lane >= o) {
+                v += t1;
+                v2 += t2;
+            }
+        }
+        if (x < fw) dst[x + 1] = make_double2(c1 + v, c2 + v2);
+        c1 += __shfl_sync(0xffffffffu, v, 31);
+        c2 += __shfl_sync(0xffffffffu, v2, 31);
     }
 }
 

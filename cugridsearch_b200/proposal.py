@@ -317,6 +317,94 @@ def serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", min_values:
     return ServeResult(params, costs, fallback, pts)
 
 
+def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", values: int = 3, levels: int = 4,
+                 spread: float = 2.0, min_half: float = 0.02, probe_values: int = 3, walks: int = 2,
+                 start=None) -> ServeResult:
+    """The learned proposal with local refinement grids (the configuration's local grid around
+    the proposal), for a batch of pairs.
+
+    1. The network's centre and radii (grid-range units) give each pair a local grid of `values`
+       values per axis over centre +- spread x radius (at least min_half of the range, clipped
+       to the full grid's range).  One persistent launch searches every pair's local grid and a
+       coarse probe of the full grid (`probe_values` full-grid values per axis).
+    2. Coarse to fine, as the reference's driver loop (src/gpu/cudaGridSearch_main_mi.cu:
+       312-363): each further launch re-centres every pair's grid on its best point with half the
+       range, `levels` times; a best point on an edge of the local grid that is not the full
+       grid's edge re-centres it without halving (at most `walks` times per pair).
+    3. A pair's answer is its best refined point; where that costs more than the probe's best
+       the pair is searched on the full grid instead (the fallback).
+    The refined points lie between the full grid's values, so the answer can be closer to the
+    true registration than the full grid's own argmin.  start: (n, 8) parameters that replace
+    the network's centres, with min_half as the first half-range (an experiment's control: the
+    refinement started at the generator's ground truth)."""
+    from . import CudaGrid
+    n = int(fixed.shape[0])
+    d = full.g.dims
+    lo = np.array([full.g.start[a] for a in range(d)], np.float64)
+    hi = np.array([full.g.end[a] for a in range(d)], np.float64)
+    step = int(getattr(net, "max_batch", n) or n)
+    out = np.concatenate([net.forward(fixed[i:i + step], moving[i:i + step]).cpu().numpy()
+                          for i in range(0, n, step)]).astype(np.float64)
+    centre = from_units(np.clip(out[:, :d], -1.0, 1.0), lo, hi)
+    half = np.clip(spread * np.exp(np.clip(out[:, 8:8 + d], -12.0, 4.0)), min_half, 1.0) * (hi - lo) / 2.0
+    if start is not None:
+        centre = np.asarray(start, np.float64)[:, :d]
+        half = np.full((n, d), min_half) * (hi - lo) / 2.0
+
+    def local(c, h):
+        a, b = np.maximum(lo, c - h), np.minimum(hi, c + h)
+        cnt = [float(values) if b[k] > a[k] else 1.0 for k in range(d)]
+        return CudaGrid.from_ranges([float(v) for v in a], [float(v) for v in np.where(b > a, b, a)], cnt)
+
+    probe = coarse_grid(full, probe_values)
+    params = np.zeros((n, d))
+    costs = np.full(n, np.inf)
+    grids = [local(centre[i], half[i]) for i in range(n)]
+    p, c, v, pts = _batch_search(cost, fixed[np.r_[0:n, 0:n]], moving[np.r_[0:n, 0:n]], grids + [probe] * n,
+                                 fixed.device)
+    probe_cost = np.where(v[n:], c[n:], np.inf)
+    left_levels = np.full(n, levels)
+    left_walks = np.full(n, walks)
+    active = np.arange(n)
+    cur_p, cur_c, cur_v, cur_g = p[:n], c[:n], v[:n], grids
+    while True:
+        nxt, ngrids = [], []
+        for j, i in enumerate(active):
+            if cur_v[j] and cur_c[j] < costs[i]:
+                params[i], costs[i] = cur_p[j], cur_c[j]
+            if not cur_v[j] or not np.isfinite(costs[i]):
+                continue
+            g = cur_g[j]
+            a = np.array([g.g.start[k] for k in range(d)], np.float64)
+            r = np.array([g.g.resolution[k] for k in range(d)], np.float64)
+            cnt = np.array([int(g.g.count[k]) for k in range(d)])
+            loc = np.where(cnt > 1, np.rint((params[i] - a) / np.where(r != 0, r, 1.0)), 0).astype(np.int64)
+            edge = ((loc == 0) & (a > lo + 1e-9 * (hi - lo))) | \
+                   ((loc == cnt - 1) & (a + r * (cnt - 1) < hi - 1e-9 * (hi - lo)))
+            if edge.any() and left_walks[i] > 0:
+                left_walks[i] -= 1
+            elif left_levels[i] > 0:
+                left_levels[i] -= 1
+                half[i] = half[i] / 2.0
+            else:
+                continue
+            nxt.append(i)
+            ngrids.append(local(params[i], half[i]))
+        if not nxt:
+            break
+        active = np.array(nxt)
+        cur_p, cur_c, cur_v, k = _batch_search(cost, fixed[active], moving[active], ngrids, fixed.device)
+        cur_g = ngrids
+        pts += k
+    fallback = ~(costs <= probe_cost)
+    if fallback.any():
+        fi = np.flatnonzero(fallback)
+        pf, cf, _, k = _batch_search(cost, fixed[fi], moving[fi], [full] * len(fi), fixed.device)
+        pts += k
+        params[fi], costs[fi] = pf, cf
+    return ServeResult(params, costs, fallback, pts)
+
+
 def corner_error(p_a, p_b, side: int = 256) -> np.ndarray:
     """Mean distance (px) between the image corners mapped by the homographies of parameter
     vectors p_a and p_b (centred parametrisation at side / 2), per row."""
@@ -365,7 +453,7 @@ def train(net: ProposalNet, fixed, moving, labels_u, epochs: int, batch: int = 2
 def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, label_side: int = 128,
                min_values: int = 3, max_values: int = 5, batch: int = 256, checkpoint: str | None = None,
                variants=None, init: str | None = None, labels: str = "grid", lr: float = 1e-3,
-               judge: str | None = None, log=print) -> dict:
+               judge: str | None = None, mode: str = "lattice", log=print) -> dict:
     """The learned-proposal configuration end to end on the current GPU: generate training pairs
     (256 px), label them -- labels="grid": the full 6^8 ZNCC grid's argmin on the pairs box-averaged
     to label_side; labels="truth": the generator's ground-truth parameters, no search -- train, then
@@ -457,24 +545,42 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
            "label_seconds": round(t_label, 1), "train_seconds": round(t_train, 1),
            "full_grid_pairs_per_s": n_eval / t_full,
            "gt_corner_error_full_grid_px": float(corner_error(truth, gte.numpy(), 256).mean()),
+           "mode": mode,
            "checkpoint": ckpt, "variants": []}
-    for (mn, mx, walks, starts) in variants or [(min_values, max_values, 6, 2)]:
-        serve(net, fe[:8], me[:8], full, min_values=mn, max_values=mx, walks=walks, starts=starts)  # warm-up
+    for var in variants or [(min_values, max_values, 6, 2)]:
+        if mode == "refine":
+            vals, lev, spread, mh, walks = var[:5]
+            kw = dict(values=int(vals), levels=int(lev), spread=float(spread), min_half=float(mh), walks=int(walks))
+            fn, desc = refine_serve, {"mode": "refine", **kw}
+            if len(var) > 5 and var[5]:  # control: refinement started at the ground truth
+                gt_np = gte.numpy()
+                desc["start"] = "ground truth"
+                fn = (lambda net_, f_, m_, full_, **k_: refine_serve(
+                    net_, f_, m_, full_, start=gt_np[:f_.shape[0]], **k_))
+        else:
+            mn, mx, walks, starts = var
+            kw = dict(min_values=mn, max_values=mx, walks=walks, starts=starts)
+            fn, desc = serve, {"mode": "lattice", **kw}
+        fn(net, fe[:8], me[:8], full, **kw)  # warm-up
         ev[0].record()
-        r = serve(net, fe, me, full, min_values=mn, max_values=mx, walks=walks, starts=starts)
+        r = fn(net, fe, me, full, **kw)
         ev[1].record()
         torch.cuda.synchronize()
         t_serve = ev[0].elapsed_time(ev[1]) / 1e3
         err = corner_error(r.params, truth, 256)
         gap = r.costs - tcost
+        gerr = corner_error(r.params, gte.numpy(), 256)
+        perr = np.abs(to_units(r.params, full.matrix()[0], full.matrix()[1]) -
+                      to_units(gte.numpy(), full.matrix()[0], full.matrix()[1])).mean(axis=0)
         res["variants"].append({
-            "min_values": mn, "max_values": mx, "walks": walks, "starts": starts,
-            "proposal_pairs_per_s": n_eval / t_serve, "speedup": t_full / t_serve,
+            **desc, "proposal_pairs_per_s": n_eval / t_serve, "speedup": t_full / t_serve,
+            "gt_corner_error_mean_px": float(gerr.mean()), "gt_corner_error_p90_px": float(np.percentile(gerr, 90)),
+            "cost_not_above_full_grid": float(np.mean(gap <= 0.0)),
+            "gt_param_error_units": [round(float(v), 5) for v in perr],
             "fallback_rate": float(r.fallback.mean()), "corner_error_mean_px": float(err.mean()),
             "corner_error_p90_px": float(np.percentile(err, 90)), "agree_within_0_5px": float(np.mean(err <= 0.5)),
             "cost_gap_mean": float(np.mean(gap)), "cost_gap_max": float(np.max(gap)),
-            "points_fraction": r.points / (n_eval * full.numElements()),
-            "gt_corner_error_px": float(corner_error(r.params, gte.numpy(), 256).mean())})
+            "points_fraction": r.points / (n_eval * full.numElements())})
         log(json.dumps(res["variants"][-1]))
     res["wall_seconds"] = round(time.time() - t0, 1)
     with open(os.path.join(out_dir, "proposal_eval.json"), "w") as fh:
@@ -510,15 +616,22 @@ if __name__ == "__main__":
     ap.add_argument("--checkpoint", default=None, help="evaluate this trained network instead of training")
     ap.add_argument("--init", default=None, help="start training from this network's parameters")
     ap.add_argument("--label-side", type=int, default=128, help="image side the labels are searched at")
-    ap.add_argument("--variants", default="3,3,6,1;3,3,6,2;3,5,6,1;3,5,6,2",
-                    help="serving variants min_values,max_values,walks,starts separated by ';'")
+    ap.add_argument("--mode", default="lattice", choices=["lattice", "refine"],
+                    help="lattice: walkers on windows of the full grid; refine: coarse-to-fine local grids")
+    ap.add_argument("--variants", default=None,
+                    help="serving variants separated by ';': lattice min_values,max_values,walks,starts; "
+                         "refine values,levels,spread,min_half,walks")
     ap.add_argument("--labels", default="grid", choices=["grid", "truth"],
                     help="grid: full-grid argmins at --label-side; truth: the generator's parameters")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--judge", default=None, help=".npz of the full grid's argmins of the held-out pairs (reused "
                                                   "when it matches --eval and --seed, else written)")
     a = ap.parse_args()
-    vs = [tuple(int(x) for x in v.split(",")) for v in a.variants.split(";") if v]
+    spec = a.variants or ("3,3,6,1;3,3,6,2;3,5,6,1;3,5,6,2" if a.mode == "lattice" else "3,4,2,0.02,2;3,5,2,0.02,2")
+    vs = [tuple(float(x) for x in v.split(",")) for v in spec.split(";") if v]
+    if a.mode == "lattice":
+        vs = [tuple(int(x) for x in v) for v in vs]
     print(json.dumps(experiment(a.train, a.eval, a.epochs, a.seed, a.out, label_side=a.label_side,
                                 min_values=a.min_values, max_values=a.max_values, checkpoint=a.checkpoint,
-                                variants=vs, init=a.init, labels=a.labels, lr=a.lr, judge=a.judge)))
+                                variants=vs, init=a.init, labels=a.labels, lr=a.lr, judge=a.judge,
+                                mode=a.mode)))

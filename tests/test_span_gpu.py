@@ -8,7 +8,10 @@ test_gpu_parity.py) and against the FP64 oracle:
   FP32 summation tolerance, on ragged sizes (moving image smaller or larger than the fixed one,
   widths that are not multiples of the tile width);
 * bit-identical costs for 2 and 4 points per warp and for the locality and the reference order;
-* every tile shape (32, 64 or 128 columns by 8, 16 or 32 rows) within tolerance;
+* every tile shape (64, 128 or 256 columns by 8, 16 or 32 rows) within tolerance;
+* maps whose rows run along the moving image's edges (no rotation, unit scale, whole-pixel
+  translations: whole rows and columns on the overlap's boundary take the exact path) against
+  the per-sample kernel and the oracle;
 * windows too large for a stage (forced small with CGS_SPAN_CAP) read global memory instead, with
   bit-identical costs;
 * the self-checking build (CGS_SPAN_CHECK=1) finds every fast sample's quad inside its window.
@@ -107,7 +110,7 @@ def test_span_tunings_bit_identical(cuda, lib):
         assert r.index == base.index
 
 
-@pytest.mark.parametrize("tx", [1, 2, 4])
+@pytest.mark.parametrize("tx", [2, 4, 8])
 @pytest.mark.parametrize("th", [8, 16, 32])
 def test_span_tile_shapes(cuda, lib, tx, th):
     pair = S.small_pair(317, size=136, count=3, cost="ZNCC", msize=128)
@@ -137,3 +140,21 @@ def test_span_config1_self_check(cuda, lib):
     with _env(CGS_SPAN_CHECK=1):
         _, c1 = _run(cuda, pair)
     np.testing.assert_array_equal(c1.view(np.uint32), c0.view(np.uint32))
+
+
+def test_span_rows_along_the_edges(cuda, lib):
+    """Translations by whole pixels (and a half pixel), no rotation, unit scale: mapped
+    coordinates land exactly on the moving image's first and last rows and columns, so whole
+    rows of the band take the reference's exact sequence."""
+    pair = S.small_pair(331, size=72, count=3, cost="ZNCC", msize=64)
+    pair.lo[:] = [0.0, 1.0, 1.0, 0.0, -8.0, -8.0, 0.0, 0.0]
+    pair.hi[:] = [0.0, 1.0, 1.0, 0.0, 8.0, 8.0, 0.0, 0.0]
+    pair.count[:] = [1, 1, 1, 1, 33, 33, 1, 1]
+    with _env(CGS_SPAN_CHECK=1):
+        res, c = _run(cuda, pair)
+    _, c0 = _per_sample(cuda, pair)
+    _agree(c, c0)
+    g = O.make_grid(*pair.grid_args())
+    c32, c64 = O.search("ZNCC", g, O.Image(pair.moving), O.Image(pair.fixed))
+    bad = close_costs(c, c32, c64, "ZNCC")
+    assert not bad.any(), int(bad.sum())
