@@ -324,6 +324,71 @@ def measure_batch(dev, rank: int, world: int, n_pairs: int, steps: int, warmup: 
             "autotune": tune}
 
 
+PROPOSAL_CHECKPOINT = os.path.join(ROOT, "models", "proposal_net.npz")
+PROPOSAL_SERVING = dict(values=3, levels=4, spread=2.0, min_half=0.02, walks=2)
+
+
+def measure_proposal(dev, n_pairs: int = 64, seed: int = 20261203 + 10 ** 7) -> dict:
+    """The learned proposal against the full grid on held-out pairs of the learned-proposal
+    configuration (256 px, full 6^8 zero-mean NCC grid): both paths timed with CUDA events on the
+    same device-resident pairs (network, refinement launches, orchestration and fallbacks
+    included), and end to end with the pairs copied in from pinned host memory; corner errors
+    against the generator's ground truth and against the full grid's argmin."""
+    import torch
+    from cugridsearch_b200 import proposal as P
+
+    fe, me, gt = P.config4_batch_cached(seed, n_pairs, dev)
+    fh, mh = fe.cpu().pin_memory(), me.cpu().pin_memory()
+    net = P.ProposalNet(max_batch=256)
+    net.load(PROPOSAL_CHECKPOINT)
+    full = P.full_grid(256, 6)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        e1.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    P.refine_serve(net, fe[:8], me[:8], full, **PROPOSAL_SERVING)  # warm-up
+    with ClockSampler(dev.index or 0) as clk:
+        (truth, tcost), t_full = timed(lambda: P.grid_argmins(fe, me, full))
+        r, t_prop = timed(lambda: P.refine_serve(net, fe, me, full, **PROPOSAL_SERVING))
+
+        def e2e():
+            fe.copy_(fh, non_blocking=True)
+            me.copy_(mh, non_blocking=True)
+            return P.refine_serve(net, fe, me, full, **PROPOSAL_SERVING)
+        r2, t_e2e = timed(e2e)
+    clocks = clk.summary()
+    net.close()
+    g = gt.numpy()
+    err_gt = P.corner_error(r.params, g, 256)
+    err_full_gt = P.corner_error(truth, g, 256)
+    err_vs_full = P.corner_error(r.params, truth, 256)
+    gap = r.costs - tcost
+    return {"pairs": n_pairs, "checkpoint": os.path.relpath(PROPOSAL_CHECKPOINT, ROOT), "serving": PROPOSAL_SERVING,
+            "full_grid_pairs_per_s": n_pairs / t_full, "proposal_pairs_per_s": n_pairs / t_prop,
+            "speedup": t_full / t_prop, "fallback_rate": float(r.fallback.mean()),
+            "corner_error_vs_ground_truth_px": {"proposal_mean": float(err_gt.mean()),
+                                                "proposal_p90": float(np.percentile(err_gt, 90)),
+                                                "full_grid_mean": float(err_full_gt.mean())},
+            "corner_error_vs_full_grid_px": {"mean": float(err_vs_full.mean()),
+                                             "p90": float(np.percentile(err_vs_full, 90))},
+            "cost_not_above_full_grid": float(np.mean(gap <= 0.0)), "cost_gap_mean": float(gap.mean()),
+            "points_fraction": r.points / (n_pairs * full.numElements()),
+            "e2e": {"value": n_pairs / t_e2e, "unit": "pairs/s",
+                    "h2d_bytes_per_step": int(fh.numel() * 4 + mh.numel() * 4),
+                    "d2h_bytes_per_step": int(r2.d2h_bytes)},
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
+                       "samples": clocks["samples"]},
+            "status_ok": bool(np.all(np.isfinite(r.costs))),
+            "workload": "learned-proposal: held-out 256x256 f32 pairs (config-4 generator), rotation +-20 deg, "
+                        "translation +-32 px; full grid 6^8 zero-mean NCC; proposal = CNN centre and radii, then "
+                        "coarse-to-fine local grids of 3 values per axis, full-grid fallback above the coarse probe"}
+
+
 def batch_bench(args):
     """The batched workload as the bench line itself (--workload batch)."""
     import torch
@@ -556,6 +621,9 @@ def main():
         line["batch"] = measure_batch(dev, rank, world, args.pairs, steps=1, warmup=1)
         line["batch"]["workload"] = WORKLOADS["batch"]
         line["batch"].pop("autotune", None)
+        # the learned proposal against the full grid (second half of the metric)
+        if os.path.exists(PROPOSAL_CHECKPOINT):
+            line["proposal"] = measure_proposal(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(pair, "NCC_REF" if cost in ("ZNCC", "NCC_REF") else cost)

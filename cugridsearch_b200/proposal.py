@@ -172,6 +172,7 @@ class ServeResult:
     costs: np.ndarray    # (n,) their costs
     fallback: np.ndarray # (n,) True where the full grid was searched
     points: int          # grid points evaluated in total (proposal + probe + fallbacks)
+    d2h_bytes: int = 0   # device-to-host bytes read back (network outputs, per-launch results)
 
 
 def full_grid(side: int = 256, values: int = 6):
@@ -360,6 +361,8 @@ def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", valu
     params = np.zeros((n, d))
     costs = np.full(n, np.inf)
     grids = [local(centre[i], half[i]) for i in range(n)]
+    rbytes = C.sizeof(_abi.CgsArgmin)
+    d2h = out.size * 4 + 2 * n * rbytes
     p, c, v, pts = _batch_search(cost, fixed[np.r_[0:n, 0:n]], moving[np.r_[0:n, 0:n]], grids + [probe] * n,
                                  fixed.device)
     probe_cost = np.where(v[n:], c[n:], np.inf)
@@ -396,13 +399,15 @@ def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", valu
         cur_p, cur_c, cur_v, k = _batch_search(cost, fixed[active], moving[active], ngrids, fixed.device)
         cur_g = ngrids
         pts += k
+        d2h += len(ngrids) * rbytes
     fallback = ~(costs <= probe_cost)
     if fallback.any():
         fi = np.flatnonzero(fallback)
         pf, cf, _, k = _batch_search(cost, fixed[fi], moving[fi], [full] * len(fi), fixed.device)
         pts += k
+        d2h += len(fi) * rbytes
         params[fi], costs[fi] = pf, cf
-    return ServeResult(params, costs, fallback, pts)
+    return ServeResult(params, costs, fallback, pts, d2h)
 
 
 def corner_error(p_a, p_b, side: int = 256) -> np.ndarray:
@@ -453,7 +458,7 @@ def train(net: ProposalNet, fixed, moving, labels_u, epochs: int, batch: int = 2
 def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, label_side: int = 128,
                min_values: int = 3, max_values: int = 5, batch: int = 256, checkpoint: str | None = None,
                variants=None, init: str | None = None, labels: str = "grid", lr: float = 1e-3,
-               judge: str | None = None, mode: str = "lattice", log=print) -> dict:
+               judge: str | None = None, mode: str = "lattice", scene: bool = False, log=print) -> dict:
     """The learned-proposal configuration end to end on the current GPU: generate training pairs
     (256 px), label them -- labels="grid": the full 6^8 ZNCC grid's argmin on the pairs box-averaged
     to label_side; labels="truth": the generator's ground-truth parameters, no search -- train, then
@@ -485,7 +490,7 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
     lo_e, hi_e = full_grid(256, 6).matrix()[0], full_grid(256, 6).matrix()[1]
     for i in range(0, n_train, chunk):
         k = min(chunk, n_train - i)
-        f, m, gt = config4_batch_cached(seed + i, k, dev)
+        f, m, gt = config4_batch_cached(seed + i, k, dev, scene)
         fd, md = downsample(f, s), downsample(m, s)
         torch.cuda.synchronize()
         if labels == "truth":
@@ -513,12 +518,12 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
         del F, M
     # evaluation at 256 px: the full grid (the judge) once, then each serving variant
     full = full_grid(256, 6)
-    fe, me, gte = config4_batch_cached(seed + 10 ** 7, n_eval, dev)
+    fe, me, gte = config4_batch_cached(seed + 10 ** 7, n_eval, dev, scene)
     ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cached = None
     if judge and os.path.exists(judge):
         z = np.load(judge)
-        if int(z["n_eval"]) == n_eval and int(z["seed"]) == seed:
+        if int(z["n_eval"]) == n_eval and int(z["seed"]) == seed and bool(z.get("scene", False)) == scene:
             cached = z
     if cached is not None:
         truth, tcost = cached["truth"], cached["cost"]
@@ -535,12 +540,13 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
         torch.cuda.synchronize()
         t_full = ev[0].elapsed_time(ev[1]) / 1e3
         if judge:
-            np.savez(judge, truth=truth, cost=tcost, n_eval=n_eval, seed=seed)
+            np.savez(judge, truth=truth, cost=tcost, n_eval=n_eval, seed=seed, scene=scene)
     # how often the label resolution's argmin is the evaluation resolution's
     lab_e, _ = grid_argmins(downsample(fe, 256 // label_side), downsample(me, 256 // label_side), full_l)
     same = np.all(np.isclose(to_units(lab_e, lo_l, hi_l), to_units(truth, full.matrix()[0], full.matrix()[1]),
                              atol=1e-4), axis=1)
     res = {"n_train": n_train, "n_eval": n_eval, "epochs": epochs, "label_side": label_side, "labels": labels,
+           "scene": scene,
            "label_matches_eval_argmin": float(same.mean()), "loss_first": hist[0], "loss_last": hist[-1],
            "label_seconds": round(t_label, 1), "train_seconds": round(t_train, 1),
            "full_grid_pairs_per_s": n_eval / t_full,
@@ -589,13 +595,13 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
     return res
 
 
-def config4_batch_cached(seed: int, n: int, device):
+def config4_batch_cached(seed: int, n: int, device, scene: bool = False):
     """config4_batch in chunks of at most 256 pairs (bounded generator memory)."""
     import torch
     from .synthetic import config4_batch
     fs, ms, gs = [], [], []
     for i in range(0, n, 256):
-        f, m, g = config4_batch(seed + i, min(256, n - i), device)
+        f, m, g = config4_batch(seed + i, min(256, n - i), device, scene=scene)
         fs.append(f)
         ms.append(m)
         gs.append(g)
@@ -624,6 +630,8 @@ if __name__ == "__main__":
     ap.add_argument("--labels", default="grid", choices=["grid", "truth"],
                     help="grid: full-grid argmins at --label-side; truth: the generator's parameters")
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--scene", action="store_true",
+                    help="moving images see the fixed image's mirror continuation past its edges (no black borders)")
     ap.add_argument("--judge", default=None, help=".npz of the full grid's argmins of the held-out pairs (reused "
                                                   "when it matches --eval and --seed, else written)")
     a = ap.parse_args()
@@ -634,4 +642,4 @@ if __name__ == "__main__":
     print(json.dumps(experiment(a.train, a.eval, a.epochs, a.seed, a.out, label_side=a.label_side,
                                 min_values=a.min_values, max_values=a.max_values, checkpoint=a.checkpoint,
                                 variants=vs, init=a.init, labels=a.labels, lr=a.lr, judge=a.judge,
-                                mode=a.mode)))
+                                mode=a.mode, scene=a.scene)))

@@ -215,13 +215,18 @@ def config4_ranges(side: int = 256):
     return _ranges(20, 0.1, 0.05, 32 * f, 1e-4 / f)
 
 
-def config4_batch(seed: int, n: int, device, side: int = 256):
+def config4_batch(seed: int, n: int, device, side: int = 256, scene: bool = False):
     """n pairs of the learned-proposal configuration generated on the GPU with torch (training
     and evaluation data; same distribution as config4(), not the same numbers): 40 blobs with
     sigma 12-40 px (at 256 px) plus the sinusoid texture, the moving image m(q) = f(H q) for a
     ground-truth H drawn uniformly in the grid ranges (centred parametrisation), Gaussian noise
     sigma 2, clipped to [0, 255].  Returns (fixed, moving, gt) as float32 tensors of shapes
-    (n, side, side), (n, side, side), (n, 8)."""
+    (n, side, side), (n, side, side), (n, 8).
+
+    scene=False: f is the fixed image, zero outside it, so the moving image is black where H q
+    leaves the fixed image.  scene=True: f continues beyond the fixed image's edges as its
+    mirror image (reflection padding by half a side), so every moving pixel sees content; the
+    fixed images are the same."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(int(seed))
     u = lambda *shape: torch.rand(*shape, generator=g, dtype=torch.float64)
@@ -247,20 +252,23 @@ def config4_batch(seed: int, n: int, device, side: int = 256):
     ty = torch.sin(2 * math.pi * yy / ly.float().to(dev)[:, None, None] + ph[:, 1].float().to(dev)[:, None, None])
     img += 0.2 * 255.0 * 0.5 * (1 + tx * ty)
     fixed = img.clamp_(0, 255)
+    margin = side // 2 if scene else 0
+    cs = side + 2 * margin
+    canvas = (torch.nn.functional.pad(fixed[:, None], (margin,) * 4, mode="reflect")[:, 0] if scene else fixed)
     H = torch.tensor(np.stack([homography(p, "centred", side / 2.0, side / 2.0) for p in gt.numpy()]),
                      dtype=torch.float32, device=dev)
     X = H[:, 0, 0, None, None] * xx + H[:, 0, 1, None, None] * yy + H[:, 0, 2, None, None]
     Y = H[:, 1, 0, None, None] * xx + H[:, 1, 1, None, None] * yy + H[:, 1, 2, None, None]
     Z = H[:, 2, 0, None, None] * xx + H[:, 2, 1, None, None] * yy + H[:, 2, 2, None, None]
-    x, y = X / Z, Y / Z
+    x, y = X / Z + margin, Y / Z + margin  # canvas coordinates
     x0, y0 = torch.floor(x), torch.floor(y)
     ax, ay = x - x0, y - y0
-    pad = torch.nn.functional.pad(fixed, (1, 1, 1, 1))
+    pad = torch.nn.functional.pad(canvas, (1, 1, 1, 1))
     ix, iy = x0.long() + 1, y0.long() + 1
-    ok = (ix >= 0) & (iy >= 0) & (ix < side + 1) & (iy < side + 1)
-    ixc, iyc = ix.clamp(0, side), iy.clamp(0, side)
+    ok = (ix >= 0) & (iy >= 0) & (ix < cs + 1) & (iy < cs + 1)
+    ixc, iyc = ix.clamp(0, cs), iy.clamp(0, cs)
     flat = pad.reshape(n, -1)
-    w2 = side + 2
+    w2 = cs + 2
 
     def tap(dy, dx):
         return torch.gather(flat, 1, ((iyc + dy) * w2 + ixc + dx).reshape(n, -1)).reshape(n, side, side)

@@ -11,6 +11,9 @@
   with blind proposals the fallback finds them anyway.
 * A short training run: the trained network lowers the held-out loss and, served, evaluates
   fewer grid points than the full grid while agreeing with it.
+* Coarse-to-fine refinement serving: started at the full grid's argmin it never loses it; with
+  the committed trained network its answers cost no more than the full grid's and lie closer to
+  the ground truth than the full grid's argmin, where an untrained network does not.
 """
 import numpy as np
 import pytest
@@ -151,3 +154,60 @@ def test_training_gains_over_untrained(cuda, lib):
         assert frac < 1.0
     finally:
         net.close()
+
+
+def test_refinement_from_the_argmin_never_loses_it(cuda, lib):
+    """Coarse-to-fine local grids started at the full grid's argmin (narrow first range): every
+    answer costs at most the argmin's cost (the start is the first grid's centre), and no pair
+    falls back."""
+    from cugridsearch_b200 import proposal as P
+
+    class Blind:
+        def forward(self, f, m):
+            import torch
+            return torch.zeros((f.shape[0], 16))
+
+    side, n = 128, 6
+    f, m, _ = _images(cuda, n, side, seed=91)
+    full = P.full_grid(side, 4)
+    truth, tcost = P.grid_argmins(f, m, full)
+    r = P.refine_serve(Blind(), f, m, full, values=3, levels=3, min_half=0.01, walks=1, start=truth)
+    assert not r.fallback.any()
+    assert np.all(r.costs <= tcost + 1e-5 * np.maximum(1.0, np.abs(tcost))), (r.costs, tcost)
+    assert r.points < n * full.numElements()
+    assert r.d2h_bytes > 0
+
+
+def test_trained_network_gains_in_refinement_serving(cuda, lib):
+    """The committed network (models/proposal_net.npz, trained on 200,000 generated pairs) on 32
+    held-out 256 px pairs, served by coarse-to-fine local grids: its answers cost no more than
+    the full grid's argmin on nearly every pair and lie closer to the generator's ground truth
+    than the full grid's argmin; an untrained network with the same serving lands far from the
+    truth or falls back."""
+    import os
+    from cugridsearch_b200 import proposal as P
+    ckpt = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "models", "proposal_net.npz")
+    n = 32
+    f, m, gt = P.config4_batch_cached(20261203 + 10 ** 7, n, cuda)
+    full = P.full_grid(256, 6)
+    truth, tcost = P.grid_argmins(f, m, full)
+    kw = dict(values=3, levels=4, spread=2.0, min_half=0.02, walks=2)
+    net = P.ProposalNet(max_batch=256)
+    raw = P.ProposalNet(max_batch=256, seed=3)
+    try:
+        net.load(ckpt)
+        r = P.refine_serve(net, f, m, full, **kw)
+        r0 = P.refine_serve(raw, f, m, full, **kw)
+    finally:
+        net.close()
+        raw.close()
+    g = gt.numpy()
+    e_trained = P.corner_error(r.params, g, 256).mean()
+    e_full = P.corner_error(truth, g, 256).mean()
+    e_raw = P.corner_error(r0.params, g, 256).mean()
+    print(f"corner error vs ground truth: trained {e_trained:.2f} px, untrained {e_raw:.2f} px, "
+          f"full grid {e_full:.2f} px; fallback {r.fallback.mean():.3f} / {r0.fallback.mean():.3f}")
+    assert r.fallback.mean() <= 1.0 / n
+    assert np.mean(r.costs <= tcost + 1e-6) >= 0.9
+    assert e_trained < 0.5 * e_full
+    assert e_trained < 0.5 * e_raw or r0.fallback.mean() > 0.25
