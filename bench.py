@@ -360,7 +360,9 @@ def measure_proposal(dev, n_pairs: int = 64, seed: int = 20261203 + 10 ** 7) -> 
             fe.copy_(fh, non_blocking=True)
             me.copy_(mh, non_blocking=True)
             return P.refine_serve(net, fe, me, full, **PROPOSAL_SERVING)
-        r2, t_e2e = timed(e2e)
+        e2e_runs = [timed(e2e) for _ in range(3)]
+        r2, t_e2e = min(e2e_runs, key=lambda v: v[1])
+        r3, t_prop2 = timed(lambda: P.refine_serve(net, fe, me, full, **PROPOSAL_SERVING))
     clocks = clk.summary()
     net.close()
     g = gt.numpy()
@@ -378,6 +380,9 @@ def measure_proposal(dev, n_pairs: int = 64, seed: int = 20261203 + 10 ** 7) -> 
                                              "p90": float(np.percentile(err_vs_full, 90))},
             "cost_not_above_full_grid": float(np.mean(gap <= 0.0)), "cost_gap_mean": float(gap.mean()),
             "points_fraction": r.points / (n_pairs * full.numElements()),
+            "timing_runs_s": {"proposal": [round(t_prop, 4), round(t_prop2, 4)],
+                              "e2e": [round(v[1], 4) for v in e2e_runs],
+                              "e2e_fallbacks": [int(v[0].fallback.sum()) for v in e2e_runs]},
             "e2e": {"value": n_pairs / t_e2e, "unit": "pairs/s",
                     "h2d_bytes_per_step": int(fh.numel() * 4 + mh.numel() * 4),
                     "d2h_bytes_per_step": int(r2.d2h_bytes)},
