@@ -441,7 +441,7 @@ def main():
     ap.add_argument("--grid-counts", default=None,
                     help="values per axis, comma-separated, in place of the workload's (profiling captures)")
     ap.add_argument("--per-sample-decisions", action="store_true",
-                    help="ZNCC on the per-sample decision kernel instead of the span kernel")
+                    help="ZNCC and MI on the per-sample decision kernel instead of the span kernels")
     ap.add_argument("--taps", default="auto", choices=["auto", "quad", "texture"],
                     help="tap source of the fast path (auto: the library's choice)")
     ap.add_argument("--workload", default="ncc", choices=["ncc", "mi", "sad", "batch"],
@@ -558,8 +558,8 @@ def main():
     h2d = mov_h.numel() * mov_h.element_size() + fix_h.numel() * fix_h.element_size()
     d2h = costs_h.numel() * 4 + res_h.numel()
 
-    span_kernel = (cost == "ZNCC" and not args.per_sample_decisions and args.taps != "texture" and
-                   pair.fixed.shape[2] == 1)
+    span_kernel = (((cost == "ZNCC" and args.taps != "texture") or (cost == "MI" and args.taps == "auto")) and
+                   not args.per_sample_decisions and pair.fixed.shape[2] == 1)
     # ---- roofline of the dominant kernel (the search kernel; staging and the FP64 verification
     # pass are well under 1% of a call)
     traffic, traffic_src = (recorded_traffic(args.workload) if cost == "ZNCC" and not args.small and
@@ -590,7 +590,7 @@ def main():
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_total / args.steps},
-            # per search: staging, (the span kernel's row prefix sums,) search, verification band, re-scoring
+            # per search: staging, (the span kernels' staging step,) search, verification band, re-scoring
             "gpu_launches": (5 if span_kernel else 4) * args.steps,
             "roofline": roofline,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],

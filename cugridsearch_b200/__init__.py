@@ -237,8 +237,8 @@ def search(cost: str, moving: CudaImage, fixed: CudaImage, grid: CudaGrid, costs
     returns the :class:`Argmin`.  ``exact_samples``: None = the cost's default (exact for
     the reference functors, fast for ZNCC / MI), True / False force a mode.  ``quad_taps``:
     None = the library's choice, True = pre-gathered 16-byte quads, False = texture gathers.
-    ``per_sample_decisions``: run single-channel ZNCC on the per-sample decision kernel instead of
-    the span kernel (CGS_FLAG_PER_SAMPLE_DECISIONS).  ``verify``: run the FP64 verification pass
+    ``per_sample_decisions``: run single-channel ZNCC and MI on the per-sample decision kernel
+    instead of the span kernels (CGS_FLAG_PER_SAMPLE_DECISIONS).  ``verify``: run the FP64 verification pass
     (the Argmin's *_fp64 fields); False sets CGS_FLAG_NO_VERIFY."""
     opt = _options(cost, mi_bins, overlap_gate, points_per_warp, warps_per_block, natural_order, exact_samples,
                    quad_taps, per_sample_decisions, verify)

@@ -71,6 +71,7 @@ struct SearchParams {
     // (the tile's fixed rows, then its window), window row pitch modulo 8
     int32_t tile_h, tiles_x, tiles_y, win_cap, win_pitch_mod;
     const double2 *fix_prefix;    // span kernel: FP64 {sum f, sum f^2} prefix sums of each fixed row, W + 1 per row
+    const float *span_rows;       // MI span kernel: the fixed bins times (B + 1), int32, the fixed plane's pitch
     // cost options
     int32_t mi_bins;
     float gate_n;        // minimum overlap terms for ZNCC / MI
@@ -289,7 +290,41 @@ __device__ __forceinline__ float zncc_cost(const double *a, int n, const SearchP
     return (float)(-cov / sqrt(vf * vm));
 }
 
-// ---------------------------------------------------------------- grid decode
+// MI cost of histogram h (B x B counts, row = fixed bin, with a marginal row and column at
+// index B; row stride `hstride`) over n terms; one warp, every lane calls it.  The marginals
+// are written into h.  The pixel-loop and span kernels share it, so equal counts give equal
+// costs.
+__device__ __forceinline__ float mi_from_hist(uint32_t *h, int n, int B, int hstride, const SearchParams &p) {
+    const int lane = threadIdx.x & 31;
+    // marginals: fixed (row sums) into column B, moving (column sums) into row B
+    for (int i = lane; i < B; i += 32) {
+        uint32_t rs = 0, cs = 0;
+        for (int j = 0; j < B; j++) {
+            rs += h[i * hstride + j];
+            cs += h[j * hstride + i];
+        }
+        h[i * hstride + B] = rs;
+        h[B * hstride + i] = cs;
+    }
+    __syncwarp();
+    const float nf = (float)n;
+    float s = 0.0f;
+    for (int j = lane; j < B; j += 32) {
+        const float hm = (float)h[B * hstride + j];
+        for (int i = 0; i < B; i++) {
+            const uint32_t v = h[i * hstride + j];
+            if (v) {
+                const float vf = (float)v;
+                const float hf = (float)h[i * hstride + B];
+                s += vf * log2f((vf * nf) / (hf * hm));
+            }
+        }
+    }
+    s = warp_sum(s);
+    return (n == 0 || nf < p.gate_n) ? __int_as_float(0x7f800000) : -s / p.total_terms;
+}
+
+// ---------------------------------------------------------------- grid decode// ---------------------------------------------------------------- grid decode
 
 // Ordinal in the evaluation order -> grid index and per-axis indices.
 __device__ __forceinline__ uint32_t ordinal_to_index(const SearchParams &p, uint32_t o, int32_t *ax) {
@@ -880,36 +915,7 @@ __device__ __forceinline__ bool run_task(const SearchParams &p, uint32_t task, c
     }
 
     // ---- per grid point: reduce, finalise, dump, argmin key ----
-    // Final MI cost of histogram h (B x B counts plus a marginal row and column) over n terms;
-    // one warp.
-    auto mi_cost = [&](uint32_t *h, int n) -> float {
-        // marginals: fixed (row sums) into column B, moving (column sums) into row B
-        for (int i = lane; i < B; i += 32) {
-            uint32_t rs = 0, cs = 0;
-            for (int j = 0; j < B; j++) {
-                rs += h[i * hstride + j];
-                cs += h[j * hstride + i];
-            }
-            h[i * hstride + B] = rs;
-            h[B * hstride + i] = cs;
-        }
-        __syncwarp();
-        const float nf = (float)n;
-        float s = 0.0f;
-        for (int j = lane; j < B; j += 32) {
-            const float hm = (float)h[B * hstride + j];
-            for (int i = 0; i < B; i++) {
-                const uint32_t v = h[i * hstride + j];
-                if (v) {
-                    const float vf = (float)v;
-                    const float hf = (float)h[i * hstride + B];
-                    s += vf * log2f((vf * nf) / (hf * hm));
-                }
-            }
-        }
-        s = warp_sum(s);
-        return (n == 0 || nf < p.gate_n) ? __int_as_float(0x7f800000) : -s / p.total_terms;
-    };
+    auto mi_cost = [&](uint32_t *h, int n) -> float { return mi_from_hist(h, n, B, hstride, p); };
 
     unsigned long long kk = ~0ull;
     if constexpr (!BSPLIT) {

@@ -724,6 +724,31 @@ bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o,
     return sp->smem <= budget;
 }
 
+// Launch plan of the MI span kernel: 16 warps of 2 points, bands of TH = 16 rows (CGS_SPAN_TH
+// = 8 | 16 | 32), self-checking with CGS_SPAN_CHECK=1.  False where it does not apply: several
+// channels, more than 32 bins (the histograms of 32 points must fit shared memory), images of
+// 32768 or more pixels a side or moving images with (W + 8) H of 2^22 or more.
+bool span_mi_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, int mi_bins, SpanPlan *sp) {
+    if (fix.channels != 1 || mi_bins > 32 || mov.width >= 32768 || mov.height >= 32768 || fix.width >= 32768 ||
+        fix.height >= 32768 || (int64_t)(mov.width + 8) * mov.height >= span_max_quads())
+        return false;
+    (void)o;
+    sp->G = 2;
+    sp->NW = 16;
+    sp->TX = 1;
+    sp->TH = env_int("CGS_SPAN_TH", 16);
+    if (!(sp->TH == 8 || sp->TH == 16 || sp->TH == 32)) return false;
+    sp->check = env_int("CGS_SPAN_CHECK", 0) != 0;
+    sp->kfn = kernel_span_mi(sp->NW, sp->check);
+    if (!sp->kfn) return false;
+    sp->tiles_x = 1;
+    sp->tiles_y = (fix.height + sp->TH - 1) / sp->TH;
+    sp->cap = 0;
+    sp->pitch_mod = 0;
+    sp->smem = span_mi_kernel_smem(sp->NW, sp->TH, mi_bins);
+    return sp->smem <= 227 * 1024;
+}
+
 // The scanline functors: staging with both images aliased, the calcMIAlt row table, one warp
 // per grid point.  Arguments are validated by cgs_search.
 static cgs_status search_scanline(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid,
@@ -933,12 +958,17 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     // taps: pre-gathered quads where the fast sampling path runs (measured faster than texture
     // gathers there); texture gathers (MI: scalar loads) for exact sampling and for MI
     const bool fast_path = !exact_samples(cost, o.flags) && cost != CGS_COST_MI;
-    const bool quads = (o.flags & CGS_FLAG_QUAD_TAPS) || (fast_path && !(o.flags & CGS_FLAG_TEXTURE_TAPS));
-    // zero-mean NCC on the fast path: the span kernel (row decisions, shared-memory windows)
+    // zero-mean NCC and MI on the fast path: the span kernels (row decisions; ZNCC with
+    // shared-memory windows, MI with shared-memory histograms); both read span-form quads
     SpanPlan sp;
-    const bool span = cost == CGS_COST_ZNCC && fast_path && quads && !(o.flags & CGS_FLAG_PER_SAMPLE_DECISIONS) &&
+    const bool per_sample = (o.flags & CGS_FLAG_PER_SAMPLE_DECISIONS) != 0;
+    const bool span = cost == CGS_COST_ZNCC && fast_path && !(o.flags & CGS_FLAG_TEXTURE_TAPS) && !per_sample &&
                       span_plan(*mov, *fix, o, &sp);
-    const void *kfn = span ? sp.kfn : getter(C, pl.G, pl.NW, quads);
+    const bool span_mi = cost == CGS_COST_MI && !exact_samples(cost, o.flags) && !per_sample &&
+                         !(o.flags & (CGS_FLAG_TEXTURE_TAPS | CGS_FLAG_QUAD_TAPS)) &&
+                         span_mi_plan(*mov, *fix, o, mi_bins, &sp);
+    const bool quads = (o.flags & CGS_FLAG_QUAD_TAPS) || (fast_path && !(o.flags & CGS_FLAG_TEXTURE_TAPS)) || span_mi;
+    const void *kfn = (span || span_mi) ? sp.kfn : getter(C, pl.G, pl.NW, quads);
     if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no kernel for this channel count / tuning");
 
     DeviceInfo di;
@@ -956,11 +986,11 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     // staged layout
     const Staging st = staging_layout(*mov, *fix, di.tex_align, di.tex_pitch_align, false, false, quads);
     const int64_t stage_bytes = set_chunks(&p, st, C, fix->height);
-    const size_t smem = span ? sp.smem
-                             : cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes,
-                                              acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
+    const size_t smem = (span || span_mi) ? sp.smem
+                                          : cta_smem_bytes(pl.G, pl.NW, (size_t)stage_bytes,
+                                                           acc_bytes(cost, pl.G, pl.NW, false, mi_bins));
     if (smem > 227 * 1024) return fail(CGS_ERROR_UNSUPPORTED, "shared-memory plan exceeds 227 KB");
-    if (span) {
+    if (span || span_mi) {
         p.tile_h = sp.TH;
         p.tiles_x = sp.tiles_x;
         p.tiles_y = sp.tiles_y;
@@ -970,14 +1000,18 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
 
     cudaMemPool_t pool;
     if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
-    // the span kernel's row prefix sums follow the staging block: W_f + 1 FP64 pairs per row
+    // the span kernels' tables follow the staging block: the ZNCC kernel's row prefix sums (W_f + 1
+    // FP64 pairs per row), the MI kernel's fixed bins (int32, the fixed plane's pitch)
     const size_t prefix_off = (size_t)round_up((int64_t)(st.bytes - (size_t)di.tex_align), 256);
-    const size_t prefix_bytes = span ? (size_t)fix->height * (size_t)(fix->width + 1) * sizeof(double2) : 0;
+    const size_t prefix_bytes = span      ? (size_t)fix->height * (size_t)(fix->width + 1) * sizeof(double2)
+                                : span_mi ? (size_t)fix->height * (size_t)st.fpitch * sizeof(int32_t)
+                                          : 0;
     void *scratch = nullptr;
-    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes + (span ? prefix_bytes + 256 : 0), pool, stream),
+    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes + (prefix_bytes ? prefix_bytes + 256 : 0), pool, stream),
              "cudaMallocFromPoolAsync");
     char *sb = staging_origin(scratch, di.tex_align);
     if (span) p.fix_prefix = reinterpret_cast<const double2 *>(sb + prefix_off);
+    if (span_mi) p.span_rows = reinterpret_cast<const float *>(sb + prefix_off);
     p.key = reinterpret_cast<unsigned long long *>(sb);
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
@@ -1012,7 +1046,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     if (quads) {
         q.quad_dst = reinterpret_cast<float4 *>(sb + st.quad_off);
         q.qplane = st.qplane;
-        q.quad_form = span ? 1 : 0;
+        q.quad_form = (span || span_mi) ? 1 : 0;
     }
     const int64_t prep_elems = (st.mplane + st.fplane) * C;
     const int prep_blocks = (int)std::min<int64_t>((prep_elems + 255) / 256, (int64_t)di.sms * 8);
@@ -1024,17 +1058,20 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     if (e == cudaSuccess && span)
         e = launch_span_prep(fstage, st.fpitch, fix->width, fix->height, const_cast<double2 *>(p.fix_prefix),
                              reinterpret_cast<float4 *>(sb + st.quad_off), st.qplane, p.shifts, stream);
+    if (e == cudaSuccess && span_mi)
+        e = launch_span_prep_mi(fstage, st.fpitch, fix->width, fix->height, mi_bins,
+                                reinterpret_cast<int32_t *>(sb + prefix_off), stream);
     if (e != cudaSuccess) {
         if (vblock) cudaFreeAsync(vblock, stream);
         cudaFreeAsync(scratch, stream);
         return cuda_fail(e, "prep_kernel");
     }
 
-    const int threads = (span ? sp.NW : pl.NW) * 32;
-    const uint32_t per_task = span ? (uint32_t)(sp.NW * sp.G) : (uint32_t)(pl.NW * pl.G);
+    const int threads = ((span || span_mi) ? sp.NW : pl.NW) * 32;
+    const uint32_t per_task = (span || span_mi) ? (uint32_t)(sp.NW * sp.G) : (uint32_t)(pl.NW * pl.G);
     p.num_tasks = (p.n + per_task - 1) / per_task;
     e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess && !span)
+    if (e == cudaSuccess && !span && !span_mi)
         e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxL1);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);

@@ -737,10 +737,9 @@ __global__ void __launch_bounds__(NW * 32, 1) span_kernel(const __grid_constant_
 // 0 .. x - 1 of row y (channel 0; one warp per row, a warp scan per 32 pixels carried in order,
 // so the sums are the same in every run); the other blocks subtract the moving image's shift
 // from every quad's constant term, so that the sweep's bilinear values are shifted already.
-__global__ void __launch_bounds__(256) span_prep_kernel(const float *__restrict__ fix, int fpitch, int fw, int fh,
-                                                        double2 *__restrict__ prefix, int row_blocks,
-                                                        float4 *__restrict__ quads, int64_t nquads,
-                                                        const float *__restrict__ shifts) {
+static __global__ void __launch_bounds__(256)
+span_prep_kernel(const float *__restrict__ fix, int fpitch, int fw, int fh, double2 *__restrict__ prefix,
+                 int row_blocks, float4 *__restrict__ quads, int64_t nquads, const float *__restrict__ shifts) {
     if ((int)blockIdx.x >= row_blocks) {
         const float ms = shifts[1];
         const int64_t nthr = (int64_t)(gridDim.x - row_blocks) * blockDim.x;

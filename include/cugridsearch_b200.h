@@ -103,10 +103,11 @@ typedef struct cgs_options {
  * only speed and scratch size differ. */
 #define CGS_FLAG_QUAD_TAPS 8
 #define CGS_FLAG_TEXTURE_TAPS 16
-/* Zero-mean NCC on the fast path runs the span kernel by default (single channel, quad taps):
- * in/out decisions per image row, taps read from per-tile moving-image windows in shared
- * memory.  This flag selects the per-sample decision kernel instead.  Both make the same
- * decisions and form the same samples; costs agree within FP32 summation order. */
+/* Zero-mean NCC and MI on the fast path run span kernels by default (single channel; MI with
+ * at most 32 bins and neither taps flag): in/out decisions per image row; ZNCC reads its taps
+ * from per-block moving-image windows in shared memory, MI keeps its histograms there.  This
+ * flag selects the per-sample decision kernel instead.  Both make the same decisions and form
+ * the same bins: ZNCC costs agree within FP32 summation order, MI costs are bit-identical. */
 #define CGS_FLAG_PER_SAMPLE_DECISIONS 32
 /* Skip the FP64 verification pass (see cgs_argmin).  Without the pass the verification fields
  * read verified = 0, index_fp64 = -1, cost_fp64 = NaN. */
