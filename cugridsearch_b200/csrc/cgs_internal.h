@@ -115,10 +115,12 @@ struct SpanPlan {
 };
 bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, SpanPlan *sp);
 // Span kernel of MI (cgs_span_mi.cuh): 2 points per warp, NW warps, histograms of B <= 32 bins;
-// its shared-memory size and its staging step (the fixed bins times B + 1, int32).
+// its shared-memory size and its staging step (the fixed bins times B + 1, int32; the quads'
+// largest slope bound into a header word).
 const void *kernel_span_mi(int NW, bool check);
 size_t span_mi_kernel_smem(int NW, int TH, int B);
-cudaError_t launch_span_prep_mi(const float *fix, int fpitch, int fw, int fh, int B, int32_t *bins, cudaStream_t stream);
+cudaError_t launch_span_prep_mi(const float *fix, int fpitch, int fw, int fh, int B, int32_t *bins,
+                                const float4 *quads, int64_t nquads, unsigned int *lmax, cudaStream_t stream);
 bool span_mi_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, int mi_bins, SpanPlan *sp);
 
 // FP64 verification pass (cgs_verify.cu): band collection and re-scoring after a search whose

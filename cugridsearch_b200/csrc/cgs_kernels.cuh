@@ -72,6 +72,7 @@ struct SearchParams {
     int32_t tile_h, tiles_x, tiles_y, win_cap, win_pitch_mod;
     const double2 *fix_prefix;    // span kernel: FP64 {sum f, sum f^2} prefix sums of each fixed row, W + 1 per row
     const float *span_rows;       // MI span kernel: the fixed bins times (B + 1), int32, the fixed plane's pitch
+    const float *span_rows_header;  // MI span kernel: the quads' largest slope bound (written by its staging step)
     // cost options
     int32_t mi_bins;
     float gate_n;        // minimum overlap terms for ZNCC / MI

@@ -1011,7 +1011,10 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
              "cudaMallocFromPoolAsync");
     char *sb = staging_origin(scratch, di.tex_align);
     if (span) p.fix_prefix = reinterpret_cast<const double2 *>(sb + prefix_off);
-    if (span_mi) p.span_rows = reinterpret_cast<const float *>(sb + prefix_off);
+    if (span_mi) {
+        p.span_rows = reinterpret_cast<const float *>(sb + prefix_off);
+        p.span_rows_header = reinterpret_cast<const float *>(sb + 32);  // zeroed with the header
+    }
     p.key = reinterpret_cast<unsigned long long *>(sb);
     p.done = reinterpret_cast<unsigned int *>(sb + 8);
     p.status = reinterpret_cast<unsigned int *>(sb + 12);
@@ -1060,7 +1063,9 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
                              reinterpret_cast<float4 *>(sb + st.quad_off), st.qplane, p.shifts, stream);
     if (e == cudaSuccess && span_mi)
         e = launch_span_prep_mi(fstage, st.fpitch, fix->width, fix->height, mi_bins,
-                                reinterpret_cast<int32_t *>(sb + prefix_off), stream);
+                                reinterpret_cast<int32_t *>(sb + prefix_off),
+                                reinterpret_cast<const float4 *>(sb + st.quad_off), st.qplane,
+                                reinterpret_cast<unsigned int *>(sb + 32), stream);
     if (e != cudaSuccess) {
         if (vblock) cudaFreeAsync(vblock, stream);
         cudaFreeAsync(scratch, stream);

@@ -15,9 +15,9 @@ const void *kernel_span_mi(int NW, bool check) {
 size_t span_mi_kernel_smem(int NW, int TH, int B) { return span_mi_smem_bytes(NW, TH, B); }
 
 cudaError_t launch_span_prep_mi(const float *fix, int fpitch, int fw, int fh, int B, int32_t *bins,
-                                cudaStream_t stream) {
-    const int blocks = (int)std::min<int64_t>(((int64_t)fh * fpitch + 255) / 256, 1024);
-    span_prep_mi_kernel<<<blocks, 256, 0, stream>>>(fix, fpitch, fw, fh, B, bins);
+                                const float4 *quads, int64_t nquads, unsigned int *lmax, cudaStream_t stream) {
+    const int blocks = (int)std::min<int64_t>((std::max<int64_t>((int64_t)fh * fpitch, nquads) + 255) / 256, 1024);
+    span_prep_mi_kernel<<<blocks, 256, 0, stream>>>(fix, fpitch, fw, fh, B, bins, quads, nquads, lmax);
     return cudaGetLastError();
 }
 
