@@ -636,10 +636,24 @@ __device__ __forceinline__ bool run_span_task(const SearchParams &p, uint32_t ta
             }
 #pragma unroll 1
             for (int c = cu0; c < cf0; c++) block(c, std::true_type{});
+            int c = cf0;
 #pragma unroll 1
-            for (int c = cf0; c <= cf1; c++) block(c, std::false_type{});
+            for (; c + 1 <= cf1; c += 2) {  // two full blocks of the same kind as straight-line code
+                const bool s0 = twin[c].w > 0, s1 = twin[c + 1].w > 0;
+                if (s0 && s1) {
+                    column(c, std::false_type{}, std::true_type{});
+                    column(c + 1, std::false_type{}, std::true_type{});
+                } else if (!s0 && !s1) {
+                    column(c, std::false_type{}, std::false_type{});
+                    column(c + 1, std::false_type{}, std::false_type{});
+                } else {
+                    block(c, std::false_type{});
+                    block(c + 1, std::false_type{});
+                }
+            }
+            if (c <= cf1) block(c, std::false_type{});
 #pragma unroll 1
-            for (int c = cf1 + 1; c <= cu1; c++) block(c, std::true_type{});
+            for (int c2 = cf1 + 1; c2 <= cu1; c2++) block(c2, std::true_type{});
         };
         for (int r = 0; r < TH; r++) {
             if (y0 + r >= fh) break;
