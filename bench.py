@@ -51,8 +51,9 @@ UNIT = "grid-point evals/s"
 # DRAM bytes per launch of the dominant kernel come from an ncu capture recorded in
 # profiles/traffic.json together with a hash of the kernel sources it was taken on; the bench
 # reports the figure only while the sources still hash the same (otherwise null).
-KERNEL_SOURCES = ["cugridsearch_b200/csrc/cgs_span.cuh", "cugridsearch_b200/csrc/cgs_kernels.cuh",
-                  "cugridsearch_b200/csrc/cgs_device.cuh", "cugridsearch_b200/csrc/cgs_search.cu"]
+KERNEL_SOURCES = ["cugridsearch_b200/csrc/cgs_span.cuh", "cugridsearch_b200/csrc/cgs_span_mi.cuh",
+                  "cugridsearch_b200/csrc/cgs_kernels.cuh", "cugridsearch_b200/csrc/cgs_device.cuh",
+                  "cugridsearch_b200/csrc/cgs_search.cu"]
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
 
 
@@ -562,9 +563,10 @@ def main():
                    not args.per_sample_decisions and pair.fixed.shape[2] == 1)
     # ---- roofline of the dominant kernel (the search kernel; staging and the FP64 verification
     # pass are well under 1% of a call)
-    traffic, traffic_src = (recorded_traffic(args.workload) if cost == "ZNCC" and not args.small and
-                            not args.grid_counts and not args.per_sample_decisions and args.taps == "auto"
-                            else (None, "no capture recorded for this configuration"))
+    traffic, traffic_src = (recorded_traffic(args.workload)
+                            if ((args.workload == "ncc" and cost == "ZNCC") or (args.workload == "mi" and cost == "MI"))
+                            and not args.small and not args.grid_counts and not args.per_sample_decisions
+                            and args.taps == "auto" else (None, "no capture recorded for this configuration"))
     flops = FLOPS_PER_PIXEL_EVAL.get(cost, 36) * n * pix
     achieved = flops / (ms_per_step / 1e3) / 1e12
     props = torch.cuda.get_device_properties(dev)
