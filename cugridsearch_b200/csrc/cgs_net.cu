@@ -8,8 +8,9 @@
 // 128 -> 16 (8 centres in [-1, 1] grid-range units, 8 log-radii).
 //
 // Numerics.  Activations are NHWC BF16, weights FP32 masters with BF16 copies; every
-// convolution (forward, data gradient, weight gradient) is an implicit GEMM on the BF16 tensor
-// cores (mma.sync m16n8k16, FP32 accumulation); pooling, the MLP, the loss and Adam run in FP32.
+// convolution is an implicit GEMM on the BF16 tensor cores with FP32 accumulation: the forward
+// on tcgen05 (UMMA, TMEM accumulators; conv_fwd_umma_kernel), the data and weight gradients on
+// mma.sync m16n8k16; pooling, the MLP, the loss and Adam run in FP32.
 //
 // Loss.  Laplace negative log-likelihood of the label y per parameter: |c - y| e^-s + s with
 // s clamped to [-6, 4] (no gradient outside), averaged over batch and parameters.
@@ -19,6 +20,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -197,6 +199,263 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(const bf16 *__restri
                     *reinterpret_cast<__nv_bfloat162 *>(y + (int64_t)m * g.Cout + co) = __floats2bfloat162_rn(v0, v1);
                 }
             }
+}
+
+// ---------------------------------------------------------------- forward on tcgen05 (UMMA)
+//
+// The forward convolution as an implicit GEMM on the 5th-generation tensor cores: D[m][co] =
+// sum_k A[m][k] B[co][k], m = (b, ho, wo) output pixels, k = (tap, ci).  A (gathered, im2col)
+// and B (the BF16 weights, [Cout][Kp]) are staged in shared memory by the CTA's 512 threads
+// with cp.async; one thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M = 128, N =
+// the CTA's channels, Cout or 64, K = 16 per instruction) into a TMEM accumulator of N columns,
+// completion tracked by tcgen05.commit on an mbarrier per stage (two stages: the next K slice is
+// gathered while the tensor cores work on the current one).  The epilogue reads the accumulator
+// back with tcgen05.ld (warp w owns TMEM lanes 32 (w % 4) .. + 31, i.e. output rows, and every
+// fourth group of 32 columns from w / 4), adds the bias, applies ReLU and stores BF16.
+//
+// Shared-memory operands use the UMMA K-major layout without swizzle: 16-byte chunks of 8
+// consecutive k of one row, chunk (row, kc) at 16 (kc * ROWS + row) bytes, so 8 consecutive
+// rows of a chunk column form one 128-byte core matrix; descriptor strides: between row
+// groups of 8 (SBO) 128 bytes, between the two 8-k halves of a K = 16 instruction (LBO)
+// 16 ROWS bytes.
+constexpr int kUmmaM = 128, kUmmaBK = 64;  // rows per tile, k per stage (up to four K = 16 instructions)
+constexpr int kUmmaT = 512;                 // threads per CTA: 4 per output row for the gathers
+
+// 16-byte global -> shared copy (cp.async, L2 only); bytes = 0 fills the 16 bytes with zeros.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(bytes)
+                 : "memory");
+}
+
+// Shared-memory matrix descriptor: start address, leading and stride byte offsets (16-byte
+// units), descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+template <int N>
+__global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
+                                                            const float *__restrict__ bias, bf16 *__restrict__ y,
+                                                            const ConvGeom g, unsigned int *__restrict__ status) {
+    static_assert(N % 16 == 0 && N >= 32 && N <= 256 && (N & (N - 1)) == 0, "TMEM columns: a power of two, 32..256");
+    constexpr int kA = kUmmaM * kUmmaBK * 2, kB = N * kUmmaBK * 2;  // bytes per stage
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *sA[2] = {smem, smem + kA};
+    unsigned char *sB[2] = {smem + 2 * kA, smem + 2 * kA + kB};
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * kA + 2 * kB);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+    volatile int *gave_up = reinterpret_cast<volatile int *>(tslot + 1);  // a bounded wait gave up
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int M = g.n * g.Ho * g.Ho;
+    const int m0 = blockIdx.x * kUmmaM, co0 = blockIdx.y * N;  // this CTA: rows m0.., channels co0 .. co0 + N
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        *gave_up = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tacc = *tslot;
+    const int nk = (g.Kp + kUmmaBK - 1) / kUmmaBK;  // Kp is a multiple of 32: the last slice may be half
+    constexpr uint32_t idesc = umma_idesc_bf16(kUmmaM, N);
+    // this thread's output row (its im2col row), decoded once; its chunks kc = part + 4 j
+    const int row = threadIdx.x & (kUmmaM - 1), part = threadIdx.x >> 7, m = m0 + row;
+    const bool mvalid = m < M;
+    int b = 0, ho = 0, wo = 0;
+    if (mvalid) {
+        b = m / (g.Ho * g.Ho);
+        const int r = m - b * g.Ho * g.Ho;
+        ho = r / g.Ho;
+        wo = r - ho * g.Ho;
+    }
+    // one K slice into stage st2: A chunks by cp.async (16 bytes of one tap's channels; zero
+    // fill outside the image and past K), or gathered through registers where 8 consecutive k
+    // span taps (Cin = 2: four taps of two channels; other Cin not a multiple of 8: element by
+    // element); B chunks by cp.async
+    auto load_slice = [&](int kb2, int st2) {
+        const int k0 = kb2 * kUmmaBK;
+        const int kchunks = min(kUmmaBK, g.Kp - k0) >> 3;
+#pragma unroll
+        for (int j = 0; j < kUmmaBK / 8 / (kUmmaT / kUmmaM); j++) {
+            const int kc = part + (kUmmaT / kUmmaM) * j;
+            unsigned char *dst = sA[st2] + 16 * (kc * kUmmaM + row);
+            const int k8 = k0 + kc * 8;
+            if ((g.Cin & 7) == 0) {
+                const bf16 *src = x;
+                uint32_t bytes = 0;
+                if (mvalid && kc < kchunks && k8 < g.K) {
+                    const int tap = k8 / g.Cin, ci = k8 - tap * g.Cin;
+                    const int hi = 2 * ho + tap / 3 - 1, wi = 2 * wo + tap % 3 - 1;
+                    if (hi >= 0 && hi < g.H && wi >= 0 && wi < g.H) {
+                        src = x + (((int64_t)b * g.H + hi) * g.H + wi) * g.Cin + ci;
+                        bytes = 16;
+                    }
+                }
+                cp_async16(dst, src, bytes);
+            } else if (g.Cin == 2) {
+                // 8 consecutive k = 4 taps x 2 channels: four 4-byte loads
+                uint32_t v[4] = {0u, 0u, 0u, 0u};
+                if (mvalid && kc < kchunks) {
+#pragma unroll
+                    for (int t = 0; t < 4; t++) {
+                        const int tap = (k8 >> 1) + t;
+                        if (2 * tap < g.K) {
+                            const int hi = 2 * ho + tap / 3 - 1, wi = 2 * wo + tap % 3 - 1;
+                            if (hi >= 0 && hi < g.H && wi >= 0 && wi < g.H)
+                                v[t] = *reinterpret_cast<const uint32_t *>(x + (((int64_t)b * g.H + hi) * g.H + wi) * 2);
+                        }
+                    }
+                }
+                *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
+            } else {
+                uint4 va = make_uint4(0, 0, 0, 0);
+                if (mvalid && kc < kchunks) va = im2col8(x, g, b, ho, wo, k8);
+                *reinterpret_cast<uint4 *>(dst) = va;
+            }
+        }
+        for (int c = threadIdx.x; c < N * (kUmmaBK / 8); c += kUmmaT) {
+            const int co = c % N, kc = c / N;
+            const bool v = kc < kchunks;
+            cp_async16(sB[st2] + 16 * (kc * N + co), v ? w + (int64_t)(co0 + co) * g.Kp + k0 + kc * 8 : w,
+                       v ? 16u : 0u);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    load_slice(0, 0);
+    for (int kb = 0; kb < nk; kb++) {
+        const int st = kb & 1;
+        const int kchunks = min(kUmmaBK, g.Kp - kb * kUmmaBK) >> 3;
+        if (kb + 1 < nk) {
+            // stage (kb + 1) & 1 is free once the MMAs of slice kb - 1 are done
+            if (kb >= 1 && !*gave_up &&
+                !mbar_wait_bounded(&bars[(kb + 1) & 1], (uint32_t)((kb - 1) >> 1) & 1u, kWaitLimitNs))
+                *gave_up = 1;
+            load_slice(kb + 1, (kb + 1) & 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");  // slice kb has landed
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        fence_proxy_async_smem();  // this thread's copies and stores, before the tensor cores read them
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (threadIdx.x == 0 && !*gave_up) {
+#pragma unroll
+            for (int j = 0; j < kUmmaBK / 16; j++) {
+                if (2 * j >= kchunks) break;  // a half slice: two instructions
+                const uint64_t da = umma_smem_desc(smem_addr(sA[st]) + j * 2 * 16 * kUmmaM, 16 * kUmmaM, 128);
+                const uint64_t db = umma_smem_desc(smem_addr(sB[st]) + j * 2 * 16 * N, 16 * N, 128);
+                const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tacc),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&bars[st]))
+                         : "memory");
+        }
+    }
+    // the last commit tracks every MMA issued before it
+    const int last = nk - 1;
+    if (!*gave_up && !mbar_wait_bounded(&bars[last & 1], (uint32_t)(last >> 1) & 1u, kWaitLimitNs)) *gave_up = 1;
+    const bool ok = __syncthreads_and(*gave_up == 0) != 0;  // the same decision in every warp
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        // a wait gave up: the tensor cores may still be writing the accumulator; give the last
+        // commit one more bounded wait before the columns are freed
+        if (threadIdx.x == 0) {
+            atomicOr(status, 1u);
+            mbar_wait_bounded(&bars[last & 1], (uint32_t)(last >> 1) & 1u, kWaitLimitNs);
+        }
+    } else {
+        // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its output rows) and every (T / 128)-th group
+        // of 32 columns from group w / 4
+        const int mo = m0 + 32 * (warp & 3) + lane;
+#pragma unroll 1
+        for (int c0 = 32 * (warp >> 2); c0 < N; c0 += 32 * (kUmmaT / kUmmaM)) {
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(tacc + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (mo < M) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    __nv_bfloat162 o[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int c = 8 * q + 2 * i;
+                        o[i] = __floats2bfloat162_rn(fmaxf(__uint_as_float(r[c]) + bias[co0 + c0 + c], 0.0f),
+                                                     fmaxf(__uint_as_float(r[c + 1]) + bias[co0 + c0 + c + 1], 0.0f));
+                    }
+                    *reinterpret_cast<uint4 *>(y + (int64_t)mo * g.Cout + co0 + c0 + 8 * q) =
+                        *reinterpret_cast<const uint4 *>(o);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tacc), "r"(N));
+}
+
+// Dynamic shared memory of conv_fwd_umma_kernel<N>: two stages of A and B, the barriers and the
+// TMEM address, rounded up where needed so that at most 512 / N CTAs share an SM (the TMEM
+// columns of all resident CTAs then fit; no allocation waits).  At 512 threads per CTA at most 4
+// CTAs are resident anyway.
+static size_t umma_fwd_smem(int N) {
+    const size_t need = 2 * (size_t)(kUmmaM + N) * kUmmaBK * 2 + 64;
+    const size_t per_sm = 228 * 1024, cap = (size_t)(512 / N);
+    if (cap >= (size_t)(2048 / kUmmaT)) return need;
+    const size_t floor_for_cap = per_sm / (cap + 1) + 1024;
+    return std::max(need, std::min(floor_for_cap, (size_t)227 * 1024));
+}
+
+template <int N>
+static cudaError_t launch_umma_n(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, const ConvGeom &g,
+                                 int blocks, unsigned int *status, cudaStream_t s) {
+    const size_t smem = umma_fwd_smem(N);
+    cudaError_t e = cudaFuncSetAttribute(conv_fwd_umma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    conv_fwd_umma_kernel<N><<<dim3(blocks, g.Cout / N), kUmmaT, smem, s>>>(x, w, bias, y, g, status);
+    return cudaGetLastError();
+}
+
+// The forward convolution of one layer on the tensor cores (Cout 32, 64, 128 or 256).  Layers
+// with fewer than two row tiles per SM split their channels over CTAs of 64 (the A tile is then
+// gathered once per channel tile).
+static cudaError_t launch_conv_fwd_umma(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, const ConvGeom &g,
+                                        int blocks, unsigned int *status, cudaStream_t s, int sms) {
+    const int nt = (g.Cout > 64 && blocks < 2 * sms) ? 64 : g.Cout;
+    switch (nt) {
+        case 32: return launch_umma_n<32>(x, w, bias, y, g, blocks, status, s);
+        case 64: return launch_umma_n<64>(x, w, bias, y, g, blocks, status, s);
+        case 128: return launch_umma_n<128>(x, w, bias, y, g, blocks, status, s);
+        case 256: return launch_umma_n<256>(x, w, bias, y, g, blocks, status, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 // Data gradient: dx[m][ci] = sum_{tap, co} dy[pixel reached by tap][co] wt[ci][tap][co], m =
@@ -490,6 +749,8 @@ struct cgs_net {
     float *lossp = nullptr;
     float *ws = nullptr;
     size_t ws_floats = 0;
+    unsigned int *status = nullptr;  // tcgen05 forward: bit 0 = a bounded wait gave up
+    bool fwd_mma_sync = false;       // CGS_NET_FORWARD=mma_sync: the mma.sync forward (comparisons)
 };
 
 namespace cgs {
@@ -559,6 +820,10 @@ cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
     nt->dev = di.dev;
     nt->sms = di.sms;
     nt->max_batch = max_batch;
+    {
+        const char *fv = std::getenv("CGS_NET_FORWARD");
+        nt->fwd_mma_sync = fv && std::string(fv) == "mma_sync";
+    }
     const int64_t P = nt->L.total;
     const int64_t B = max_batch;
     // sizes in bytes, each block 256-aligned
@@ -579,6 +844,7 @@ cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
     sz.push_back(((size_t)B * (2 * kFeat + 2 * kHid + 2 * kOut + 1)) * 4 + 7 * 256);
     nt->ws_floats = ws_need(max_batch, di.sms);
     sz.push_back(nt->ws_floats * 4 + 256);
+    sz.push_back(256);  // status word
     size_t total = 0;
     for (size_t v : sz) total += (v + 255) / 256 * 256;
     cudaError_t e = cudaMalloc(&nt->mem, total);
@@ -613,6 +879,7 @@ cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
     nt->dout = reinterpret_cast<float *>(take((size_t)B * kOut * 4));
     nt->lossp = reinterpret_cast<float *>(take((size_t)B * 4));
     nt->ws = reinterpret_cast<float *>(take(nt->ws_floats * 4));
+    nt->status = reinterpret_cast<unsigned int *>(take(4));
 
     // He-normal initialisation (std sqrt(2 / fan_in)); the last layer small so the first
     // proposals sit at the grid centre with radius ~1 (half the range)
@@ -630,6 +897,7 @@ cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
     if (e == cudaSuccess) e = cudaMemset(nt->m1, 0, P * 4);
     if (e == cudaSuccess) e = cudaMemset(nt->m2, 0, P * 4);
     if (e == cudaSuccess) e = cudaMemset(nt->grads, 0, P * 4);
+    if (e == cudaSuccess) e = cudaMemset(nt->status, 0, 4);
     for (int l = 1; l < kLayers && e == cudaSuccess; l++) e = cudaMemset(nt->wt[l], 0, (size_t)kCout[l] * kpad(l) * 2);
     if (e != cudaSuccess) {
         cudaFree(nt->mem);
@@ -656,6 +924,9 @@ cgs_status cgs_net_destroy(cgs_net *nt) {
 cgs_status cgs_net_get_params(const cgs_net *nt, float *host) {
     if (!nt || !host) return fail(CGS_ERROR_INVALID_VALUE, "network or buffer is null");
     CGS_CUDA(cudaMemcpy(host, nt->params, nt->L.total * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    unsigned int st = 0;
+    CGS_CUDA(cudaMemcpy(&st, nt->status, 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (st) return fail(CGS_ERROR_DEVICE_TIMEOUT, "a tensor-core forward pass gave up waiting on its barriers");
     return CGS_SUCCESS;
 }
 
@@ -689,8 +960,14 @@ cgs_status cgs_net_forward(cgs_net *nt, const float *fixed, const float *moving,
     for (int l = 0; l < kLayers; l++) {
         const ConvGeom g = geom(l, n);
         const int M = n * g.Ho * g.Ho;
-        conv_fwd_kernel<<<dim3((M + BM - 1) / BM, (g.Cout + BN - 1) / BN), kThreads, 0, s>>>(
-            nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nt->act[l + 1], g);
+        if (nt->fwd_mma_sync) {  // the warp-level mma.sync forward, kept for comparison
+            conv_fwd_kernel<<<dim3((M + BM - 1) / BM, (g.Cout + BN - 1) / BN), kThreads, 0, s>>>(
+                nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nt->act[l + 1], g);
+            continue;
+        }
+        cudaError_t e = launch_conv_fwd_umma(nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nt->act[l + 1], g,
+                                             (M + kUmmaM - 1) / kUmmaM, nt->status, s, nt->sms);
+        if (e != cudaSuccess) return cuda_fail(e, "conv_fwd_umma_kernel");
     }
     gap_kernel<<<(n * kFeat + 255) / 256, 256, 0, s>>>(nt->act[kLayers], n, nt->feat);
     fc_kernel<<<(n * kHid + 255) / 256, 256, 0, s>>>(nt->feat, nt->params + nt->L.fc1w, nt->params + nt->L.fc1b, n,
