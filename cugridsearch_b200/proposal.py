@@ -608,6 +608,38 @@ def config4_batch_cached(seed: int, n: int, device, scene: bool = False):
     return torch.cat(fs), torch.cat(ms), torch.cat(gs)
 
 
+def forward_timing(batch: int = 256, reps: int = 20, seed: int = 7) -> dict:
+    """Forward passes and training steps of the network on random 128 x 128 pairs (CUDA events,
+    after warm-up): the ms per forward and per training step at `batch` pairs."""
+    import torch
+    dev = torch.device("cuda")
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    f = (torch.rand(batch, 128, 128, generator=g) * 255).to(dev).contiguous()
+    m = (torch.rand(batch, 128, 128, generator=g) * 255).to(dev).contiguous()
+    lab = (torch.rand(batch, 8, generator=g) * 2 - 1).to(dev).contiguous()
+    net = ProposalNet(max_batch=batch, seed=seed)
+    try:
+        for _ in range(3):
+            net.forward(f, m)
+        ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev[0].record()
+        for _ in range(reps):
+            net.forward(f, m)
+        ev[1].record()
+        ev[1].synchronize()
+        fwd = ev[0].elapsed_time(ev[1]) / reps
+        ev[0].record()
+        for _ in range(reps):
+            net.train_step(f, m, lab, 1e-6)
+        ev[1].record()
+        ev[1].synchronize()
+        step = ev[0].elapsed_time(ev[1]) / reps
+        net.params()  # raises if a tensor-core pass gave up waiting
+    finally:
+        net.close()
+    return {"batch": batch, "forward_ms": fwd, "train_step_ms": step}
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -634,7 +666,12 @@ if __name__ == "__main__":
                     help="moving images see the fixed image's mirror continuation past its edges (no black borders)")
     ap.add_argument("--judge", default=None, help=".npz of the full grid's argmins of the held-out pairs (reused "
                                                   "when it matches --eval and --seed, else written)")
+    ap.add_argument("--net-timing", action="store_true",
+                    help="only time the network's forward pass and training step on random pairs")
     a = ap.parse_args()
+    if a.net_timing:
+        print(json.dumps(forward_timing()))
+        raise SystemExit(0)
     spec = a.variants or ("3,3,6,1;3,3,6,2;3,5,6,1;3,5,6,2" if a.mode == "lattice" else "3,4,2,0.02,2;3,5,2,0.02,2")
     vs = [tuple(float(x) for x in v.split(",")) for v in spec.split(";") if v]
     if a.mode == "lattice":
