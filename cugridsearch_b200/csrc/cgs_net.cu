@@ -9,8 +9,8 @@
 //
 // Numerics.  Activations are NHWC BF16, weights FP32 masters with BF16 copies; every
 // convolution is an implicit GEMM on the BF16 tensor cores with FP32 accumulation: the forward
-// on tcgen05 (UMMA, TMEM accumulators; conv_fwd_umma_kernel), the data and weight gradients on
-// mma.sync m16n8k16; pooling, the MLP, the loss and Adam run in FP32.
+// and the data gradient on tcgen05 (UMMA, TMEM accumulators; conv_umma_kernel), the weight
+// gradient on mma.sync m16n8k16; pooling, the MLP, the loss and Adam run in FP32.
 //
 // Loss.  Laplace negative log-likelihood of the label y per parameter: |c - y| e^-s + s with
 // s clamped to [-6, 4] (no gradient outside), averaged over batch and parameters.
@@ -239,10 +239,16 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-template <int N>
-__global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
-                                                            const float *__restrict__ bias, bf16 *__restrict__ y,
-                                                            const ConvGeom g, unsigned int *__restrict__ status) {
+// BWD = false: the forward, x = the layer's input, w = [Cout][Kp], y = relu(conv + bias).
+// BWD = true: the data gradient, x = the output gradient dy [n][Ho][Ho][Cout], w = the transposed
+// weights [Cin][9 Cout], mask = the previous layer's output (ReLU mask), y = dx [n][H][H][Cin]:
+// rows are input pixels, k = (tap, co), and a row's chunk reads dy at the output pixel the tap
+// reaches (none where the stride skips it).
+template <int N, bool BWD>
+__global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
+                                                           const float *__restrict__ bias,
+                                                           const bf16 *__restrict__ mask, bf16 *__restrict__ y,
+                                                           const ConvGeom g, unsigned int *__restrict__ status) {
     static_assert(N % 16 == 0 && N >= 32 && N <= 256 && (N & (N - 1)) == 0, "TMEM columns: a power of two, 32..256");
     constexpr int kA = kUmmaM * kUmmaBK * 2, kB = N * kUmmaBK * 2;  // bytes per stage
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -252,7 +258,10 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
     volatile int *gave_up = reinterpret_cast<volatile int *>(tslot + 1);  // a bounded wait gave up
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int M = g.n * g.Ho * g.Ho;
+    const int side = BWD ? g.H : g.Ho;         // rows: output pixels (forward) or input pixels
+    const int M = g.n * side * side;
+    const int KT = BWD ? 9 * g.Cout : g.Kp;   // GEMM K (a multiple of 32)
+    const int CO = BWD ? g.Cin : g.Cout;      // GEMM N: the output's channels
     const int m0 = blockIdx.x * kUmmaM, co0 = blockIdx.y * N;  // this CTA: rows m0.., channels co0 .. co0 + N
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
@@ -269,17 +278,17 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tacc = *tslot;
-    const int nk = (g.Kp + kUmmaBK - 1) / kUmmaBK;  // Kp is a multiple of 32: the last slice may be half
+    const int nk = (KT + kUmmaBK - 1) / kUmmaBK;  // KT is a multiple of 32: the last slice may be half
     constexpr uint32_t idesc = umma_idesc_bf16(kUmmaM, N);
     // this thread's output row (its im2col row), decoded once; its chunks kc = part + 4 j
     const int row = threadIdx.x & (kUmmaM - 1), part = threadIdx.x >> 7, m = m0 + row;
     const bool mvalid = m < M;
     int b = 0, ho = 0, wo = 0;
     if (mvalid) {
-        b = m / (g.Ho * g.Ho);
-        const int r = m - b * g.Ho * g.Ho;
-        ho = r / g.Ho;
-        wo = r - ho * g.Ho;
+        b = m / (side * side);
+        const int r = m - b * side * side;
+        ho = r / side;  // (hi, wi) for the data gradient
+        wo = r - ho * side;
     }
     // one K slice into stage st2: A chunks by cp.async (16 bytes of one tap's channels; zero
     // fill outside the image and past K), or gathered through registers where 8 consecutive k
@@ -287,13 +296,26 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
     // element); B chunks by cp.async
     auto load_slice = [&](int kb2, int st2) {
         const int k0 = kb2 * kUmmaBK;
-        const int kchunks = min(kUmmaBK, g.Kp - k0) >> 3;
+        const int kchunks = min(kUmmaBK, KT - k0) >> 3;
 #pragma unroll
         for (int j = 0; j < kUmmaBK / 8 / (kUmmaT / kUmmaM); j++) {
             const int kc = part + (kUmmaT / kUmmaM) * j;
             unsigned char *dst = sA[st2] + 16 * (kc * kUmmaM + row);
             const int k8 = k0 + kc * 8;
-            if ((g.Cin & 7) == 0) {
+            if constexpr (BWD) {
+                // 8 consecutive k = 8 output channels of one tap (Cout is a multiple of 8)
+                const bf16 *src = x;
+                uint32_t bytes = 0;
+                if (mvalid && kc < kchunks) {
+                    const int tap = k8 / g.Cout, co = k8 - tap * g.Cout;
+                    const int ho2 = ho + 1 - tap / 3, wo2 = wo + 1 - tap % 3;
+                    if (ho2 >= 0 && wo2 >= 0 && !(ho2 & 1) && !(wo2 & 1) && (ho2 >> 1) < g.Ho && (wo2 >> 1) < g.Ho) {
+                        src = x + (((int64_t)b * g.Ho + (ho2 >> 1)) * g.Ho + (wo2 >> 1)) * g.Cout + co;
+                        bytes = 16;
+                    }
+                }
+                cp_async16(dst, src, bytes);
+            } else if ((g.Cin & 7) == 0) {
                 const bf16 *src = x;
                 uint32_t bytes = 0;
                 if (mvalid && kc < kchunks && k8 < g.K) {
@@ -329,7 +351,7 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
         for (int c = threadIdx.x; c < N * (kUmmaBK / 8); c += kUmmaT) {
             const int co = c % N, kc = c / N;
             const bool v = kc < kchunks;
-            cp_async16(sB[st2] + 16 * (kc * N + co), v ? w + (int64_t)(co0 + co) * g.Kp + k0 + kc * 8 : w,
+            cp_async16(sB[st2] + 16 * (kc * N + co), v ? w + (int64_t)(co0 + co) * KT + k0 + kc * 8 : w,
                        v ? 16u : 0u);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -337,7 +359,7 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
     load_slice(0, 0);
     for (int kb = 0; kb < nk; kb++) {
         const int st = kb & 1;
-        const int kchunks = min(kUmmaBK, g.Kp - kb * kUmmaBK) >> 3;
+        const int kchunks = min(kUmmaBK, KT - kb * kUmmaBK) >> 3;
         if (kb + 1 < nk) {
             // stage (kb + 1) & 1 is free once the MMAs of slice kb - 1 are done
             if (kb >= 1 && !*gave_up &&
@@ -402,15 +424,27 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
             if (mo < M) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
+                    const int64_t o0 = (int64_t)mo * CO + co0 + c0 + 8 * q;
                     __nv_bfloat162 o[4];
+                    if constexpr (BWD) {  // the previous layer's ReLU mask
+                        const uint4 pv = *reinterpret_cast<const uint4 *>(mask + o0);
+                        const __nv_bfloat162 *pm = reinterpret_cast<const __nv_bfloat162 *>(&pv);
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const int c = 8 * q + 2 * i;
-                        o[i] = __floats2bfloat162_rn(fmaxf(__uint_as_float(r[c]) + bias[co0 + c0 + c], 0.0f),
-                                                     fmaxf(__uint_as_float(r[c + 1]) + bias[co0 + c0 + c + 1], 0.0f));
+                        for (int i = 0; i < 4; i++) {
+                            const float2 pf = __bfloat1622float2(pm[i]);
+                            const int c = 8 * q + 2 * i;
+                            o[i] = __floats2bfloat162_rn(pf.x > 0.0f ? __uint_as_float(r[c]) : 0.0f,
+                                                         pf.y > 0.0f ? __uint_as_float(r[c + 1]) : 0.0f);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 4; i++) {
+                            const int c = 8 * q + 2 * i;
+                            o[i] = __floats2bfloat162_rn(fmaxf(__uint_as_float(r[c]) + bias[co0 + c0 + c], 0.0f),
+                                                         fmaxf(__uint_as_float(r[c + 1]) + bias[co0 + c0 + c + 1], 0.0f));
+                        }
                     }
-                    *reinterpret_cast<uint4 *>(y + (int64_t)mo * g.Cout + co0 + c0 + 8 * q) =
-                        *reinterpret_cast<const uint4 *>(o);
+                    *reinterpret_cast<uint4 *>(y + o0) = *reinterpret_cast<const uint4 *>(o);
                 }
             }
         }
@@ -420,7 +454,7 @@ __global__ void __launch_bounds__(kUmmaT) conv_fwd_umma_kernel(const bf16 *__res
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tacc), "r"(N));
 }
 
-// Dynamic shared memory of conv_fwd_umma_kernel<N>: two stages of A and B, the barriers and the
+// Dynamic shared memory of conv_umma_kernel<N, BWD>: two stages of A and B, the barriers and the
 // TMEM address, rounded up where needed so that at most 512 / N CTAs share an SM (the TMEM
 // columns of all resident CTAs then fit; no allocation waits).  At 512 threads per CTA at most 4
 // CTAs are resident anyway.
@@ -432,28 +466,39 @@ static size_t umma_fwd_smem(int N) {
     return std::max(need, std::min(floor_for_cap, (size_t)227 * 1024));
 }
 
-template <int N>
-static cudaError_t launch_umma_n(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, const ConvGeom &g,
-                                 int blocks, unsigned int *status, cudaStream_t s) {
+template <int N, bool BWD>
+static cudaError_t launch_umma_n(const bf16 *x, const bf16 *w, const float *bias, const bf16 *mask, bf16 *y,
+                                 const ConvGeom &g, int blocks, int channels, unsigned int *status, cudaStream_t s) {
     const size_t smem = umma_fwd_smem(N);
-    cudaError_t e = cudaFuncSetAttribute(conv_fwd_umma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(conv_umma_kernel<N, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    conv_fwd_umma_kernel<N><<<dim3(blocks, g.Cout / N), kUmmaT, smem, s>>>(x, w, bias, y, g, status);
+    conv_umma_kernel<N, BWD><<<dim3(blocks, channels / N), kUmmaT, smem, s>>>(x, w, bias, mask, y, g, status);
     return cudaGetLastError();
 }
 
-// The forward convolution of one layer on the tensor cores (Cout 32, 64, 128 or 256).  Layers
-// with fewer than two row tiles per SM split their channels over CTAs of 64 (the A tile is then
-// gathered once per channel tile).
-static cudaError_t launch_conv_fwd_umma(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, const ConvGeom &g,
-                                        int blocks, unsigned int *status, cudaStream_t s, int sms) {
-    const int nt = (g.Cout > 64 && blocks < 2 * sms) ? 64 : g.Cout;
+// One layer's forward convolution (bwd = false: x, w = [Cout][Kp], bias -> y) or data gradient
+// (bwd = true: dy, w = [Cin][9 Cout], ReLU mask -> dx) on the tensor cores; output channels 32,
+// 64, 128 or 256.  Layers with fewer than two row tiles per SM split their channels over CTAs
+// of 64 (the A tile is then gathered once per channel tile).
+static cudaError_t launch_conv_umma(bool bwd, const bf16 *x, const bf16 *w, const float *bias, const bf16 *mask,
+                                    bf16 *y, const ConvGeom &g, unsigned int *status, cudaStream_t s, int sms) {
+    const int side = bwd ? g.H : g.Ho, channels = bwd ? g.Cin : g.Cout;
+    const int blocks = (g.n * side * side + kUmmaM - 1) / kUmmaM;
+    const int nt = (channels > 64 && blocks < 2 * sms) ? 64 : channels;
+    if (bwd) {
+        switch (nt) {
+            case 32: return launch_umma_n<32, true>(x, w, bias, mask, y, g, blocks, channels, status, s);
+            case 64: return launch_umma_n<64, true>(x, w, bias, mask, y, g, blocks, channels, status, s);
+            case 128: return launch_umma_n<128, true>(x, w, bias, mask, y, g, blocks, channels, status, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (nt) {
-        case 32: return launch_umma_n<32>(x, w, bias, y, g, blocks, status, s);
-        case 64: return launch_umma_n<64>(x, w, bias, y, g, blocks, status, s);
-        case 128: return launch_umma_n<128>(x, w, bias, y, g, blocks, status, s);
-        case 256: return launch_umma_n<256>(x, w, bias, y, g, blocks, status, s);
+        case 32: return launch_umma_n<32, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
+        case 64: return launch_umma_n<64, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
+        case 128: return launch_umma_n<128, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
+        case 256: return launch_umma_n<256, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -750,7 +795,7 @@ struct cgs_net {
     float *ws = nullptr;
     size_t ws_floats = 0;
     unsigned int *status = nullptr;  // tcgen05 forward: bit 0 = a bounded wait gave up
-    bool fwd_mma_sync = false;       // CGS_NET_FORWARD=mma_sync: the mma.sync forward (comparisons)
+    bool conv_mma_sync = false;      // CGS_NET_CONV=mma_sync: the mma.sync forward and data gradient (comparisons)
 };
 
 namespace cgs {
@@ -821,8 +866,8 @@ cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
     nt->sms = di.sms;
     nt->max_batch = max_batch;
     {
-        const char *fv = std::getenv("CGS_NET_FORWARD");
-        nt->fwd_mma_sync = fv && std::string(fv) == "mma_sync";
+        const char *fv = std::getenv("CGS_NET_CONV");
+        nt->conv_mma_sync = fv && std::string(fv) == "mma_sync";
     }
     const int64_t P = nt->L.total;
     const int64_t B = max_batch;
@@ -960,14 +1005,14 @@ cgs_status cgs_net_forward(cgs_net *nt, const float *fixed, const float *moving,
     for (int l = 0; l < kLayers; l++) {
         const ConvGeom g = geom(l, n);
         const int M = n * g.Ho * g.Ho;
-        if (nt->fwd_mma_sync) {  // the warp-level mma.sync forward, kept for comparison
+        if (nt->conv_mma_sync) {  // the warp-level mma.sync forward, kept for comparison
             conv_fwd_kernel<<<dim3((M + BM - 1) / BM, (g.Cout + BN - 1) / BN), kThreads, 0, s>>>(
                 nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nt->act[l + 1], g);
             continue;
         }
-        cudaError_t e = launch_conv_fwd_umma(nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nt->act[l + 1], g,
-                                             (M + kUmmaM - 1) / kUmmaM, nt->status, s, nt->sms);
-        if (e != cudaSuccess) return cuda_fail(e, "conv_fwd_umma_kernel");
+        cudaError_t e = launch_conv_umma(false, nt->act[l], nt->wb[l], nt->params + nt->L.b[l], nullptr,
+                                         nt->act[l + 1], g, nt->status, s, nt->sms);
+        if (e != cudaSuccess) return cuda_fail(e, "conv_umma_kernel (forward)");
     }
     gap_kernel<<<(n * kFeat + 255) / 256, 256, 0, s>>>(nt->act[kLayers], n, nt->feat);
     fc_kernel<<<(n * kHid + 255) / 256, 256, 0, s>>>(nt->feat, nt->params + nt->L.fc1w, nt->params + nt->L.fc1b, n,
@@ -1011,8 +1056,13 @@ cgs_status cgs_net_backward(cgs_net *nt, const float *labels, float *loss, cgs_s
         sum_splits_kernel<<<1, 256, 0, s>>>(nt->ws, chunks, g.Cout, G + nt->L.b[l]);
         if (l > 0) {
             const int Min = n * g.H * g.H;
-            conv_bwd_data_kernel<<<dim3((Min + BM - 1) / BM, (g.Cin + BN - 1) / BN), kThreads, 0, s>>>(
-                dy, nt->wt[l], nt->act[l], dx, g);
+            if (nt->conv_mma_sync) {  // the warp-level mma.sync data gradient, kept for comparison
+                conv_bwd_data_kernel<<<dim3((Min + BM - 1) / BM, (g.Cin + BN - 1) / BN), kThreads, 0, s>>>(
+                    dy, nt->wt[l], nt->act[l], dx, g);
+            } else {
+                cudaError_t e = launch_conv_umma(true, dy, nt->wt[l], nullptr, nt->act[l], dx, g, nt->status, s, nt->sms);
+                if (e != cudaSuccess) return cuda_fail(e, "conv_umma_kernel (data gradient)");
+            }
             std::swap(dy, dx);
         }
     }
