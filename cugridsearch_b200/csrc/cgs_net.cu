@@ -241,9 +241,12 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
 
 // BWD = false: the forward, x = the layer's input, w = [Cout][Kp], y = relu(conv + bias).
 // BWD = true: the data gradient, x = the output gradient dy [n][Ho][Ho][Cout], w = the transposed
-// weights [Cin][9 Cout], mask = the previous layer's output (ReLU mask), y = dx [n][H][H][Cin]:
-// rows are input pixels, k = (tap, co), and a row's chunk reads dy at the output pixel the tap
-// reaches (none where the stride skips it).
+// weights [Cin][9 Cout], mask = the previous layer's output (ReLU mask), y = dx [n][H][H][Cin].
+// With stride 2 an input pixel (hi, wi) receives only the taps ky = hi + 1 (mod 2), kx = wi + 1
+// (mod 2), so the rows are split by parity class (py, px) = (hi, wi) mod 2 (blockIdx.z, the four-tap
+// class first): a class's rows are the pixels (2i + py, 2j + px) and its K = (1 + py)(1 + px) Cout,
+// k = (t, co) over the class's taps t = (ty, tx), ky = py ? 2 ty : 1, kx = px ? 2 tx : 1, which
+// read dy at (i + py (1 - ty), j + px (1 - tx)) where that is inside the output.
 template <int N, bool BWD>
 __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
                                                            const float *__restrict__ bias,
@@ -258,10 +261,12 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
     volatile int *gave_up = reinterpret_cast<volatile int *>(tslot + 1);  // a bounded wait gave up
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int side = BWD ? g.H : g.Ho;         // rows: output pixels (forward) or input pixels
+    const int side = BWD ? g.H >> 1 : g.Ho;  // rows: output pixels, or one parity class of input pixels
     const int M = g.n * side * side;
-    const int KT = BWD ? 9 * g.Cout : g.Kp;   // GEMM K (a multiple of 32)
-    const int CO = BWD ? g.Cin : g.Cout;      // GEMM N: the output's channels
+    const int ph = BWD ? 3 - (int)blockIdx.z : 0, py = ph >> 1, px = ph & 1, ntx = 1 + px;
+    const int KT = BWD ? (1 + py) * ntx * g.Cout : g.Kp;  // GEMM K (a multiple of 32; of 64 for BWD)
+    const int wstride = BWD ? 9 * g.Cout : g.Kp;           // B row stride
+    const int CO = BWD ? g.Cin : g.Cout;                   // GEMM N: the output's channels
     const int m0 = blockIdx.x * kUmmaM, co0 = blockIdx.y * N;  // this CTA: rows m0.., channels co0 .. co0 + N
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
     if (mvalid) {
         b = m / (side * side);
         const int r = m - b * side * side;
-        ho = r / side;  // (hi, wi) for the data gradient
+        ho = r / side;  // (i, j) of the parity class for the data gradient
         wo = r - ho * side;
     }
     // one K slice into stage st2: A chunks by cp.async (16 bytes of one tap's channels; zero
@@ -297,6 +302,11 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
     auto load_slice = [&](int kb2, int st2) {
         const int k0 = kb2 * kUmmaBK;
         const int kchunks = min(kUmmaBK, KT - k0) >> 3;
+        int woff = 0;  // BWD: a slice lies inside one tap t (64 divides Cout); B reads wt's block of tap(t)
+        if constexpr (BWD) {
+            const int t = k0 / g.Cout, ty = t / ntx, tx = t - ty * ntx;
+            woff = (3 * (py ? 2 * ty : 1) + (px ? 2 * tx : 1) - t) * g.Cout;
+        }
 #pragma unroll
         for (int j = 0; j < kUmmaBK / 8 / (kUmmaT / kUmmaM); j++) {
             const int kc = part + (kUmmaT / kUmmaM) * j;
@@ -307,10 +317,10 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
                 const bf16 *src = x;
                 uint32_t bytes = 0;
                 if (mvalid && kc < kchunks) {
-                    const int tap = k8 / g.Cout, co = k8 - tap * g.Cout;
-                    const int ho2 = ho + 1 - tap / 3, wo2 = wo + 1 - tap % 3;
-                    if (ho2 >= 0 && wo2 >= 0 && !(ho2 & 1) && !(wo2 & 1) && (ho2 >> 1) < g.Ho && (wo2 >> 1) < g.Ho) {
-                        src = x + (((int64_t)b * g.Ho + (ho2 >> 1)) * g.Ho + (wo2 >> 1)) * g.Cout + co;
+                    const int t = k8 / g.Cout, co = k8 - t * g.Cout, ty = t / ntx, tx = t - ty * ntx;
+                    const int ho2 = ho + py * (1 - ty), wo2 = wo + px * (1 - tx);
+                    if (ho2 < g.Ho && wo2 < g.Ho) {
+                        src = x + (((int64_t)b * g.Ho + ho2) * g.Ho + wo2) * g.Cout + co;
                         bytes = 16;
                     }
                 }
@@ -351,8 +361,8 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
         for (int c = threadIdx.x; c < N * (kUmmaBK / 8); c += kUmmaT) {
             const int co = c % N, kc = c / N;
             const bool v = kc < kchunks;
-            cp_async16(sB[st2] + 16 * (kc * N + co), v ? w + (int64_t)(co0 + co) * KT + k0 + kc * 8 : w,
-                       v ? 16u : 0u);
+            cp_async16(sB[st2] + 16 * (kc * N + co),
+                       v ? w + (int64_t)(co0 + co) * wstride + woff + k0 + kc * 8 : w, v ? 16u : 0u);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -407,7 +417,12 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
     } else {
         // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its output rows) and every (T / 128)-th group
         // of 32 columns from group w / 4
-        const int mo = m0 + 32 * (warp & 3) + lane;
+        const int mr = m0 + 32 * (warp & 3) + lane;  // the row; its pixel mo
+        int mo = mr;
+        if constexpr (BWD) {
+            const int bb = mr / (side * side), r = mr - bb * side * side, i = r / side, j = r - i * side;
+            mo = (bb * g.H + 2 * i + py) * g.H + 2 * j + px;
+        }
 #pragma unroll 1
         for (int c0 = 32 * (warp >> 2); c0 < N; c0 += 32 * (kUmmaT / kUmmaM)) {
             uint32_t r[32];
@@ -421,7 +436,7 @@ __global__ void __launch_bounds__(kUmmaT) conv_umma_kernel(const bf16 *__restric
                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                 : "r"(tacc + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (mo < M) {
+            if (mr < M) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int64_t o0 = (int64_t)mo * CO + co0 + c0 + 8 * q;
@@ -473,7 +488,8 @@ static cudaError_t launch_umma_n(const bf16 *x, const bf16 *w, const float *bias
     cudaError_t e = cudaFuncSetAttribute(conv_umma_kernel<N, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    conv_umma_kernel<N, BWD><<<dim3(blocks, channels / N), kUmmaT, smem, s>>>(x, w, bias, mask, y, g, status);
+    conv_umma_kernel<N, BWD><<<dim3(blocks, channels / N, BWD ? 4 : 1), kUmmaT, smem, s>>>(x, w, bias, mask, y, g,
+                                                                                           status);
     return cudaGetLastError();
 }
 
@@ -483,9 +499,11 @@ static cudaError_t launch_umma_n(const bf16 *x, const bf16 *w, const float *bias
 // of 64 (the A tile is then gathered once per channel tile).
 static cudaError_t launch_conv_umma(bool bwd, const bf16 *x, const bf16 *w, const float *bias, const bf16 *mask,
                                     bf16 *y, const ConvGeom &g, unsigned int *status, cudaStream_t s, int sms) {
-    const int side = bwd ? g.H : g.Ho, channels = bwd ? g.Cin : g.Cout;
+    // the data gradient runs the four parity classes of input pixels as grid.z (stride 2, H even)
+    if (bwd && ((g.H & 1) || g.Ho != g.H / 2 || (g.Cout & 63))) return cudaErrorInvalidValue;
+    const int side = bwd ? g.H / 2 : g.Ho, channels = bwd ? g.Cin : g.Cout;
     const int blocks = (g.n * side * side + kUmmaM - 1) / kUmmaM;
-    const int nt = (channels > 64 && blocks < 2 * sms) ? 64 : channels;
+    const int nt = (channels > 64 && blocks * (bwd ? 4 : 1) < 2 * sms) ? 64 : channels;
     if (bwd) {
         switch (nt) {
             case 32: return launch_umma_n<32, true>(x, w, bias, mask, y, g, blocks, channels, status, s);
@@ -499,6 +517,232 @@ static cudaError_t launch_conv_umma(bool bwd, const bf16 *x, const bf16 *w, cons
         case 64: return launch_umma_n<64, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
         case 128: return launch_umma_n<128, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
         case 256: return launch_umma_n<256, false>(x, w, bias, mask, y, g, blocks, channels, status, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------- weight gradient on tcgen05
+//
+// D[k][co] = sum_p A[k][p] dy[p][co] for one tile of 128 im2col columns k (blockIdx.x) over the
+// pixels of one split (blockIdx.z), in slices of 64 pixels; A[k][p] = im2col(p, k) for k < K, 0
+// for K <= k < Kp, and 1 for k = Kp, so that accumulator row Kp is the bias gradient.  Both
+// operands are MN-major in shared memory: the natural 16-byte chunk (8 consecutive k, or 8
+// channels, of one pixel) is one row of a core matrix, chunk (pixel p, chunk column c) at
+// 1024 c + 16 p bytes; descriptor strides: between pixel groups of 8 (LBO, the K direction) 128
+// bytes, between chunk columns (SBO, the M / N direction) 1024 bytes.  The epilogue writes
+// part[z][co][k] (k < Kp) and partb[z][co] (k = Kp), summed over splits in a fixed order after.
+template <int N>
+__global__ void __launch_bounds__(kUmmaT) conv_wgrad_umma_kernel(const bf16 *__restrict__ dy,
+                                                                 const bf16 *__restrict__ x, float *__restrict__ part,
+                                                                 float *__restrict__ partb, const ConvGeom g,
+                                                                 int slices_per_split,
+                                                                 unsigned int *__restrict__ status) {
+    static_assert(N >= 32 && N <= 256 && (N & (N - 1)) == 0, "TMEM columns: a power of two, 32..256");
+    constexpr int kA = kUmmaM * 64 * 2, kB = N * 64 * 2;  // bytes per stage: 128 rows k / N channels x 64 pixels
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *sA[2] = {smem, smem + kA};
+    unsigned char *sB[2] = {smem + 2 * kA, smem + 2 * kA + kB};
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * kA + 2 * kB);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+    volatile int *gave_up = reinterpret_cast<volatile int *>(tslot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int P = g.n * g.Ho * g.Ho, k0 = blockIdx.x * kUmmaM;
+    const int s_begin = blockIdx.z * slices_per_split;
+    const int ns = min(slices_per_split, (P + 63) / 64 - s_begin);  // >= 1 by the launch's split count
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        *gave_up = 0;
+    }
+    // chunk columns of A past K hold the same values for every pixel: zeros, and the 1 of row Kp
+    const int pl = threadIdx.x & 63, cg = threadIdx.x >> 6;  // this thread's pixel in a slice, first chunk column
+    const int kreal = (g.K - k0 + 7) >> 3;                    // chunk columns with im2col values (may be <= 0)
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int c = cg + 8 * j;
+        if (c >= kreal) {
+            const int kb = k0 + 8 * c;
+            const uint32_t one = (g.Kp >= kb && g.Kp < kb + 8) ? 0x3F80u << (16 * ((g.Kp - kb) & 1)) : 0u;
+            const int word = (g.Kp - kb) >> 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (one) {
+                if (word == 0) v.x = one;
+                else if (word == 1) v.y = one;
+                else if (word == 2) v.z = one;
+                else v.w = one;
+            }
+            *reinterpret_cast<uint4 *>(sA[0] + 1024 * c + 16 * pl) = v;
+            *reinterpret_cast<uint4 *>(sA[1] + 1024 * c + 16 * pl) = v;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tacc = *tslot;
+    constexpr uint32_t idesc = umma_idesc_bf16(kUmmaM, N) | (1u << 15) | (1u << 16);  // A and B MN-major
+    // one slice of 64 pixels into stage st2: A's im2col chunks and B's dy chunks by cp.async
+    // (zero fill outside the image and past the last pixel), Cin = 2 through registers
+    auto load_slice = [&](int si, int st2) {
+        const int p = (s_begin + si) * 64 + pl;
+        const bool pv = p < P;
+        int b = 0, ho = 0, wo = 0;
+        if (pv) {
+            b = p / (g.Ho * g.Ho);
+            const int r = p - b * g.Ho * g.Ho;
+            ho = r / g.Ho;
+            wo = r - ho * g.Ho;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int c = cg + 8 * j;
+            if (c < kreal) {
+                unsigned char *dst = sA[st2] + 1024 * c + 16 * pl;
+                const int k8 = k0 + 8 * c;
+                if ((g.Cin & 7) == 0) {
+                    const bf16 *src = x;
+                    uint32_t bytes = 0;
+                    if (pv) {
+                        const int tap = k8 / g.Cin, ci = k8 - tap * g.Cin;
+                        const int hi = 2 * ho + tap / 3 - 1, wi = 2 * wo + tap % 3 - 1;
+                        if (hi >= 0 && hi < g.H && wi >= 0 && wi < g.H) {
+                            src = x + (((int64_t)b * g.H + hi) * g.H + wi) * g.Cin + ci;
+                            bytes = 16;
+                        }
+                    }
+                    cp_async16(dst, src, bytes);
+                } else if (g.Cin == 2) {
+                    uint32_t v[4] = {0u, 0u, 0u, 0u};
+                    if (pv) {
+#pragma unroll
+                        for (int t = 0; t < 4; t++) {
+                            const int tap = (k8 >> 1) + t;
+                            if (2 * tap < g.K) {
+                                const int hi = 2 * ho + tap / 3 - 1, wi = 2 * wo + tap % 3 - 1;
+                                if (hi >= 0 && hi < g.H && wi >= 0 && wi < g.H)
+                                    v[t] = *reinterpret_cast<const uint32_t *>(
+                                        x + (((int64_t)b * g.H + hi) * g.H + wi) * 2);
+                            }
+                        }
+                    }
+                    *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
+                } else {
+                    *reinterpret_cast<uint4 *>(dst) = pv ? im2col8(x, g, b, ho, wo, k8) : make_uint4(0, 0, 0, 0);
+                }
+            }
+        }
+        for (int c = cg; c < N / 8; c += 8)
+            cp_async16(sB[st2] + 1024 * c + 16 * pl, pv ? dy + (int64_t)p * g.Cout + 8 * c : dy, pv ? 16u : 0u);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    load_slice(0, 0);
+    for (int si = 0; si < ns; si++) {
+        const int st = si & 1;
+        if (si + 1 < ns) {
+            // stage (si + 1) & 1 is free once the MMAs of slice si - 1 are done
+            if (si >= 1 && !*gave_up &&
+                !mbar_wait_bounded(&bars[(si + 1) & 1], (uint32_t)((si - 1) >> 1) & 1u, kWaitLimitNs))
+                *gave_up = 1;
+            load_slice(si + 1, (si + 1) & 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        fence_proxy_async_smem();
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (threadIdx.x == 0 && !*gave_up) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {  // K = 16 pixels per instruction: pixel groups 2 j, 2 j + 1
+                const uint64_t da = umma_smem_desc(smem_addr(sA[st]) + 256 * j, 128, 1024);
+                const uint64_t db = umma_smem_desc(smem_addr(sB[st]) + 256 * j, 128, 1024);
+                const uint32_t acc = (si > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tacc),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&bars[st]))
+                         : "memory");
+        }
+    }
+    const int last = ns - 1;
+    if (!*gave_up && !mbar_wait_bounded(&bars[last & 1], (uint32_t)(last >> 1) & 1u, kWaitLimitNs)) *gave_up = 1;
+    const bool ok = __syncthreads_and(*gave_up == 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (threadIdx.x == 0) {
+            atomicOr(status, 1u);
+            mbar_wait_bounded(&bars[last & 1], (uint32_t)(last >> 1) & 1u, kWaitLimitNs);
+        }
+    } else {
+        const int k = k0 + 32 * (warp & 3) + lane;  // this thread's accumulator row
+        float *out = part + (int64_t)blockIdx.z * g.Cout * g.Kp;
+#pragma unroll 1
+        for (int c0 = 32 * (warp >> 2); c0 < N; c0 += 32 * (kUmmaT / kUmmaM)) {
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(tacc + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (k < g.Kp) {
+#pragma unroll
+                for (int i = 0; i < 32; i++) out[(int64_t)(c0 + i) * g.Kp + k] = __uint_as_float(r[i]);
+            } else if (k == g.Kp) {
+#pragma unroll
+                for (int i = 0; i < 32; i++) partb[(int64_t)blockIdx.z * g.Cout + c0 + i] = __uint_as_float(r[i]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tacc), "r"(N));
+}
+
+// Splits of the pixel slices for conv_wgrad_umma_kernel: about two CTAs per SM over the k tiles,
+// at least four slices per split.
+static int wgrad_umma_splits(const ConvGeom &g, int sms, int *slices_per_split) {
+    const int slices = (g.n * g.Ho * g.Ho + 63) / 64, ktiles = g.Kp / kUmmaM + 1;
+    int splits = std::max(1, std::min(slices / 4, (2 * sms + ktiles - 1) / ktiles));
+    *slices_per_split = (slices + splits - 1) / splits;
+    return (slices + *slices_per_split - 1) / *slices_per_split;
+}
+
+template <int N>
+static cudaError_t launch_wgrad_n(const bf16 *dy, const bf16 *x, float *part, float *partb, const ConvGeom &g,
+                                  int splits, int sps, unsigned int *status, cudaStream_t s) {
+    const size_t smem = umma_fwd_smem(N);
+    cudaError_t e = cudaFuncSetAttribute(conv_wgrad_umma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    conv_wgrad_umma_kernel<N><<<dim3(g.Kp / kUmmaM + 1, 1, splits), kUmmaT, smem, s>>>(dy, x, part, partb, g, sps,
+                                                                                       status);
+    return cudaGetLastError();
+}
+
+// One layer's weight and bias gradient partials on the tensor cores (Cout 32, 64, 128 or 256).
+static cudaError_t launch_conv_wgrad_umma(const bf16 *dy, const bf16 *x, float *part, float *partb,
+                                          const ConvGeom &g, int splits, int sps, unsigned int *status,
+                                          cudaStream_t s) {
+    switch (g.Cout) {
+        case 32: return launch_wgrad_n<32>(dy, x, part, partb, g, splits, sps, status, s);
+        case 64: return launch_wgrad_n<64>(dy, x, part, partb, g, splits, sps, status, s);
+        case 128: return launch_wgrad_n<128>(dy, x, part, partb, g, splits, sps, status, s);
+        case 256: return launch_wgrad_n<256>(dy, x, part, partb, g, splits, sps, status, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -622,7 +866,15 @@ __global__ void __launch_bounds__(kThreads) conv_bwd_weight_kernel(const bf16 *_
 __global__ void sum_splits_kernel(const float *__restrict__ part, int splits, int64_t n, float *__restrict__ dst) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         float s = 0.0f;
-        for (int z = 0; z < splits; z++) s += part[(int64_t)z * n + i];
+        int z = 0;
+        for (; z + 8 <= splits; z += 8) {  // eight loads in flight, added in split order
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = part[(int64_t)(z + u) * n + i];
+#pragma unroll
+            for (int u = 0; u < 8; u++) s += v[u];
+        }
+        for (; z < splits; z++) s += part[(int64_t)z * n + i];
         dst[i] = s;
     }
 }
@@ -796,6 +1048,7 @@ struct cgs_net {
     size_t ws_floats = 0;
     unsigned int *status = nullptr;  // tcgen05 forward: bit 0 = a bounded wait gave up
     bool conv_mma_sync = false;      // CGS_NET_CONV=mma_sync: the mma.sync forward and data gradient (comparisons)
+    bool wgrad_mma_sync = false;     // CGS_NET_CONV=mma_sync or CGS_NET_WGRAD=mma_sync: the mma.sync weight gradient
 };
 
 namespace cgs {
@@ -843,6 +1096,8 @@ static size_t ws_need(int n, int sms) {
         need = std::max(need, (size_t)sp * g.Cout * g.Kp);
         const int P = n * g.Ho * g.Ho, chunk = 1024;
         need = std::max(need, (size_t)((P + chunk - 1) / chunk) * g.Cout);
+        const int su = wgrad_umma_splits(g, sms, &tps);
+        need = std::max(need, (size_t)su * g.Cout * (g.Kp + 1));
     }
     return need;
 }
@@ -868,6 +1123,8 @@ cgs_status cgs_net_create(int32_t max_batch, uint64_t seed, cgs_net **out) {
     {
         const char *fv = std::getenv("CGS_NET_CONV");
         nt->conv_mma_sync = fv && std::string(fv) == "mma_sync";
+        const char *wv = std::getenv("CGS_NET_WGRAD");
+        nt->wgrad_mma_sync = nt->conv_mma_sync || (wv && std::string(wv) == "mma_sync");
     }
     const int64_t P = nt->L.total;
     const int64_t B = max_batch;
@@ -1044,16 +1301,27 @@ cgs_status cgs_net_backward(cgs_net *nt, const float *labels, float *loss, cgs_s
     bf16 *dy = nt->dya, *dx = nt->dyb;
     for (int l = kLayers - 1; l >= 0; l--) {
         const ConvGeom g = geom(l, n);
-        int tps;
-        const int splits = wgrad_splits(g, nt->sms, &tps);
-        conv_bwd_weight_kernel<<<dim3((g.Cout + BM - 1) / BM, (g.Kp + BN - 1) / BN, splits), kThreads, 0, s>>>(
-            dy, nt->act[l], nt->ws, g, tps);
         const int64_t wn = (int64_t)g.Cout * g.Kp;
-        sum_splits_kernel<<<(int)std::min<int64_t>((wn + 255) / 256, 1024), 256, 0, s>>>(nt->ws, splits, wn,
-                                                                                          G + nt->L.w[l]);
-        const int P = n * g.Ho * g.Ho, chunk = 1024, chunks = (P + chunk - 1) / chunk;
-        bias_grad_kernel<<<chunks, 256, 0, s>>>(dy, P, g.Cout, chunk, nt->ws);
-        sum_splits_kernel<<<1, 256, 0, s>>>(nt->ws, chunks, g.Cout, G + nt->L.b[l]);
+        if (nt->wgrad_mma_sync) {  // the warp-level mma.sync weight gradient, kept for comparison
+            int tps;
+            const int splits = wgrad_splits(g, nt->sms, &tps);
+            conv_bwd_weight_kernel<<<dim3((g.Cout + BM - 1) / BM, (g.Kp + BN - 1) / BN, splits), kThreads, 0, s>>>(
+                dy, nt->act[l], nt->ws, g, tps);
+            sum_splits_kernel<<<(int)std::min<int64_t>((wn + 255) / 256, 1024), 256, 0, s>>>(nt->ws, splits, wn,
+                                                                                              G + nt->L.w[l]);
+            const int P = n * g.Ho * g.Ho, chunk = 1024, chunks = (P + chunk - 1) / chunk;
+            bias_grad_kernel<<<chunks, 256, 0, s>>>(dy, P, g.Cout, chunk, nt->ws);
+            sum_splits_kernel<<<1, 256, 0, s>>>(nt->ws, chunks, g.Cout, G + nt->L.b[l]);
+        } else {
+            int sps;
+            const int splits = wgrad_umma_splits(g, nt->sms, &sps);
+            float *partb = nt->ws + (int64_t)splits * wn;
+            cudaError_t e = launch_conv_wgrad_umma(dy, nt->act[l], nt->ws, partb, g, splits, sps, nt->status, s);
+            if (e != cudaSuccess) return cuda_fail(e, "conv_wgrad_umma_kernel");
+            sum_splits_kernel<<<(int)std::min<int64_t>((wn + 255) / 256, 1024), 256, 0, s>>>(nt->ws, splits, wn,
+                                                                                              G + nt->L.w[l]);
+            sum_splits_kernel<<<(g.Cout + 255) / 256, 256, 0, s>>>(partb, splits, g.Cout, G + nt->L.b[l]);
+        }
         if (l > 0) {
             const int Min = n * g.H * g.H;
             if (nt->conv_mma_sync) {  // the warp-level mma.sync data gradient, kept for comparison
