@@ -430,16 +430,20 @@ class BatchPair:
     mi_bins: int = 0
     overlap_gate: float = 0.0
     exact_samples: bool | None = None
+    per_sample_decisions: bool = False
 
     def to_c(self) -> CgsPair:
-        opt = _options(self.cost, self.mi_bins, self.overlap_gate, exact_samples=self.exact_samples)
+        opt = _options(self.cost, self.mi_bins, self.overlap_gate, exact_samples=self.exact_samples,
+                       per_sample_decisions=self.per_sample_decisions)
         return CgsPair(self.moving.img, self.fixed.img, self.grid.g, opt,
                        self.costs.data_ptr() if self.costs is not None else None, self.result.data_ptr())
 
 
 class Batch:
-    """Many pairs in one persistent launch (cgs_batch_*): the pairs' images, dumps and
-    results are bound at creation; :meth:`launch` replays the recorded CUDA graph."""
+    """Many pairs in one recorded launch sequence (cgs_batch_*): a persistent kernel over the
+    pairs' tasks, then the span-kernel searches of the ZNCC and MI pairs that :func:`search`
+    runs on span kernels; the pairs' images, dumps and results are bound at creation;
+    :meth:`launch` replays the recorded CUDA graph."""
 
     def __init__(self, pairs: list[BatchPair], plan: BatchPlan | None = None):
         self.pairs = list(pairs)  # keeps the tensors alive
@@ -479,6 +483,13 @@ class Batch:
         a, b = (C.c_uint64 * n)(), (C.c_uint64 * n)()
         check(_abi.load().cgs_batch_pair_times(self._h, a, b))
         return np.array(list(a), dtype=np.uint64), np.array(list(b), dtype=np.uint64)
+
+    @property
+    def kernel_launches(self) -> int:
+        """Kernel launches of one :meth:`launch` (the recorded graph's kernel nodes)."""
+        n = C.c_int32(0)
+        check(_abi.load().cgs_batch_kernel_launches(self._h, C.byref(n)))
+        return int(n.value)
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

@@ -39,7 +39,7 @@ EXPORTS = [
     "cgs_mi_histogram", "cgs_search_noalloc", "cgs_covariance", "cgs_search_refine",
     "cgs_homography", "cgs_transform_image", "cgs_fuse_aligned", "cgs_filter_image", "cgs_quantize_image",
     "cgs_batch_create", "cgs_batch_launch", "cgs_batch_set_plan", "cgs_batch_get_plan", "cgs_batch_autotune",
-    "cgs_batch_pair_times", "cgs_batch_destroy", "cgs_search_batched", "cgs_autotune",
+    "cgs_batch_pair_times", "cgs_batch_kernel_launches", "cgs_batch_destroy", "cgs_search_batched", "cgs_autotune",
     "cgs_net_param_count", "cgs_net_create", "cgs_net_destroy", "cgs_net_get_params", "cgs_net_set_params",
     "cgs_net_get_grads", "cgs_net_forward", "cgs_net_backward", "cgs_net_adam_step", "cgs_grid_window",
     "cgs_proposal_window",
@@ -150,6 +150,8 @@ def load() -> C.CDLL:
                                          P(CgsBatchPlan)]
         L.cgs_batch_pair_times.restype = C.c_int
         L.cgs_batch_pair_times.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
+        L.cgs_batch_kernel_launches.restype = C.c_int
+        L.cgs_batch_kernel_launches.argtypes = [C.c_void_p, P(C.c_int32)]
         L.cgs_batch_destroy.restype = C.c_int
         L.cgs_batch_destroy.argtypes = [C.c_void_p]
         L.cgs_search_batched.restype = C.c_int

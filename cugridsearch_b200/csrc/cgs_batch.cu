@@ -1,8 +1,12 @@
 // cgs_batch.cu -- C ABI of the batched search: a handle that stages many image pairs, orders
-// their tasks, holds a CUDA graph of (clear, stage, persistent batch kernel), replays it, and
-// tunes the kernel's plan by timing candidates on a sample of every pair's grid.
+// their tasks, holds a CUDA graph of one launch sequence -- clear, stage, the persistent batch
+// kernel over the per-sample pairs, the multi-pair span kernel over the ZNCC pairs that
+// cgs_search runs on its span kernel, and cgs_search's own launches for large MI pairs that it
+// runs on the MI span kernel -- replays it, and tunes the persistent kernel's plan by timing
+// candidates on a sample of every pair's grid.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -45,17 +49,39 @@ __global__ void header_reset_kernel(char *headers, uint32_t n) {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Span-kernel tasks per SM from which an MI pair (or a ZNCC pair outside the multi-pair span
+// kernel's plan) is searched by its own span launches (CGS_BATCH_SPAN_TASKS_PER_SM overrides
+// it; 0 routes every span-eligible pair).
+constexpr uint32_t kSpanRouteTasksPerSm = 4;
+static uint32_t span_route_tasks_per_sm() {
+    const char *v = std::getenv("CGS_BATCH_SPAN_TASKS_PER_SM");
+    if (!v || !*v) return kSpanRouteTasksPerSm;
+    const long t = std::strtol(v, nullptr, 10);
+    return t < 0 ? kSpanRouteTasksPerSm : (uint32_t)std::min<long>(t, 1L << 20);
+}
+
+// %globaltimer (ns) into *t: the start and end stamps of a pair searched by its own launches.
+__global__ void stamp_kernel(unsigned long long *t) {
+    unsigned long long v;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+    *t = v;
+}
+
 }  // namespace cgs
 
 using namespace cgs;
 
 // The handle.  Device memory is one block:
-//   zeroed per launch:    headers [n x 32 B] | task counter (16 B) | t_end [n]
+//   zeroed per launch:    headers [n x 32 B] | task counter (16 B) | t_end [n] | span task counter (16 B)
 //   all ones per launch:  t_start [n]
 //   per plan:             params [n] | task_begin [n + 1]
-//   fixed:                prep params [n] | staged planes (one tex_align-aligned block per pair)
+//   fixed:                prep params [n] | span pairs' params, task_begin, stamp slots, staging
+//                         arguments | staged planes (one tex_align-aligned block per pair) | span
+//                         pairs' row prefix sums | own-launch pairs' scratch
 //   tuning:               params [n] | task_begin [n + 1] | task counter | headers [n] | results [n]
 // Pairs are kept in execution order (ascending estimated work); order[i] is the caller's index.
+// Routes (execution order): 0 the persistent kernel, 1 the multi-pair span kernel, 2 the pair's
+// own cgs_search launches.
 struct cgs_batch {
     int dev = -1;
     int sms = 0;
@@ -79,9 +105,21 @@ struct cgs_batch {
     char *t_headers = nullptr;
     cgs_argmin *t_results = nullptr;
     std::vector<cudaTextureObject_t> tex;
+    std::vector<uint8_t> route;
+    // route 2: searched after the kernels by the same launches as cgs_search, in scratch of their own
+    std::vector<cgs_pair> span_pair;
+    std::vector<size_t> span_off, span_bytes;
+    // route 1: the multi-pair span kernel's launch and staging step
+    uint32_t g_n = 0, g_blocks = 0;
+    int g_prep_blocks = 0;
+    size_t g_smem = 0;
+    const void *g_kfn = nullptr;
+    SpanBatchParams g_args{};
+    SpanPrepArgs *d_gprep = nullptr;
     cgs_batch_plan plan = {2, 16, 0, 0};
     uint32_t total_tasks = 0;
     uint32_t blocks = 0;
+    int32_t kernel_nodes = 0;  // kernel launches per replay of the graph
     size_t smem = 0;
     const void *kfn = nullptr;
     cudaStream_t cap = nullptr;
@@ -98,7 +136,10 @@ static void release(cgs_batch *b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     for (cudaTextureObject_t t : b->tex)
         if (t) cudaDestroyTextureObject(t);
-    if (b->mem) cudaFree(b->mem);
+    if (b->mem) {  // back to the pool (kept there for the next batch), in the batch's stream order
+        cudaFreeAsync(b->mem, b->cap);
+        cudaStreamSynchronize(b->cap);
+    }
     if (b->cap) cudaStreamDestroy(b->cap);
     if (b->last) cudaEventDestroy(b->last);
     delete b;
@@ -130,6 +171,7 @@ static cgs_status plan_shape(const cgs_batch &b, const cgs_batch_plan &pl, uint3
     sh->tasks.assign(b.n, 0u);
     uint64_t total = 0;
     for (uint32_t i = 0; i < b.n; i++) {
+        if (b.route[i]) continue;                               // searched by span kernels
         const int gi = batch_pair_points(b.params[i].cost, G);  // this pair's points per warp
         const uint32_t ppt = (uint32_t)(bs ? gi : gi * NW);     // points per task
         const uint32_t pts = cap ? std::min(cap, b.params[i].n) : b.params[i].n;
@@ -182,10 +224,26 @@ static cgs_status enqueue_launch(const cgs_batch &b, cudaStream_t s) {
     const PrepParams *qs = b.d_prep;
     void *pargs[] = {&qs};
     CGS_CUDA(cudaLaunchKernel(batch_prep_kernel_fn(), dim3(px, b.n), dim3(256), pargs, 0, s), "batch_prep_kernel");
+    if (b.g_n > 0) CGS_CUDA(launch_span_prep_batch(b.d_gprep, (int)b.g_n, b.g_prep_blocks, s), "span_prep_batch_kernel");
     BatchParams a = batch_args(b, false, b.total_tasks);
     void *kargs[] = {&a};
-    CGS_CUDA(cudaLaunchKernel(b.kfn, dim3(b.blocks), dim3(b.plan.warps_per_block * 32), kargs, b.smem, s),
-             "batch_kernel");
+    if (b.total_tasks > 0)
+        CGS_CUDA(cudaLaunchKernel(b.kfn, dim3(b.blocks), dim3(b.plan.warps_per_block * 32), kargs, b.smem, s),
+                 "batch_kernel");
+    if (b.g_n > 0) {
+        SpanBatchParams ga = b.g_args;
+        void *gargs[] = {&ga};
+        CGS_CUDA(cudaLaunchKernel(b.g_kfn, dim3(b.g_blocks), dim3(16 * 32), gargs, b.g_smem, s), "span_batch_kernel");
+    }
+    for (uint32_t j = 0; j < b.n; j++) {
+        if (b.route[j] != 2) continue;
+        stamp_kernel<<<1, 1, 0, s>>>(b.t_start + j);
+        CGS_CUDA(cudaGetLastError(), "stamp_kernel");
+        const cgs_status st = span_route_enqueue(b.span_pair[j], b.mem + b.span_off[j], b.span_bytes[j], s);
+        if (st != CGS_SUCCESS) return fail(st, "pair " + std::to_string(b.order[j]) + ": " + cgs_last_error());
+        stamp_kernel<<<1, 1, 0, s>>>(b.t_end + j);
+        CGS_CUDA(cudaGetLastError(), "stamp_kernel");
+    }
     return CGS_SUCCESS;
 }
 
@@ -224,6 +282,16 @@ static cgs_status apply_plan(cgs_batch *b, const cgs_batch_plan &pl) {
     }
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
     b->graph = g;
+    size_t nn = 0;
+    CGS_CUDA(cudaGraphGetNodes(b->graph, nullptr, &nn), "cudaGraphGetNodes");
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) CGS_CUDA(cudaGraphGetNodes(b->graph, nodes.data(), &nn), "cudaGraphGetNodes");
+    b->kernel_nodes = 0;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        CGS_CUDA(cudaGraphNodeGetType(nd, &t), "cudaGraphNodeGetType");
+        if (t == cudaGraphNodeTypeKernel) b->kernel_nodes++;
+    }
     CGS_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
     return CGS_SUCCESS;
 }
@@ -252,7 +320,13 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
         int mi_bins;
         int64_t stage_elems;
         bool quads = false;
+        int route = 0;
+        size_t span_bytes = 0;
+        SpanPlan zp;         // route 1: the pair's span plan
+        size_t prefix_off = 0;
     };
+    SpanPlan gplan;          // the multi-pair span kernel's plan (of its first pair)
+    bool have_group = false;
     std::vector<Pending> pend((size_t)n);
     for (int32_t i = 0; i < n; i++) {
         const cgs_pair &q = pairs[i];
@@ -273,13 +347,37 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
     }
     DeviceInfo di;
     if ((s = device_info(&di)) != CGS_SUCCESS) return s;
+    const uint64_t route_tasks = (uint64_t)span_route_tasks_per_sm() * (uint64_t)di.sms;
     for (int32_t i = 0; i < n; i++) {
         const cgs_pair &q = pairs[i];
         Pending &pd = pend[i];
-        // ZNCC pairs on the fast sampling path read pre-gathered tap quads, as single searches do
+        // ZNCC pairs that cgs_search runs on its span kernel share one multi-pair span launch
+        // (same kernel plan); other span-eligible pairs are searched by their own launches once
+        // their grid fills the GPU by itself (a few tasks per SM), and stay in the persistent
+        // kernel below that (a refinement level's local grids, balanced there many at once)
+        uint32_t ppt = 0;
+        if ((q.options.cost == CGS_COST_ZNCC || q.options.cost == CGS_COST_MI) &&
+            span_route_bytes(q, &pd.span_bytes, &ppt)) {
+            SpanPlan zp;
+            const bool grouped = q.options.cost == CGS_COST_ZNCC && span_plan(q.moving, q.fixed, q.options, &zp) &&
+                                 kernel_span_zncc_batch(zp.G, zp.NW, zp.TX, zp.check) != nullptr &&
+                                 (!have_group || (zp.G == gplan.G && zp.NW == gplan.NW && zp.TX == gplan.TX &&
+                                                  zp.TH == gplan.TH && zp.pitch_mod == gplan.pitch_mod));
+            if (grouped) {
+                pd.route = 1;
+                pd.zp = zp;
+                if (!have_group) gplan = zp;
+                have_group = true;
+            } else if ((uint64_t)pd.p.n >= route_tasks * ppt) {
+                pd.route = 2;
+            }
+        }
+        // ZNCC pairs of the persistent kernel on the fast sampling path read pre-gathered tap
+        // quads, as single searches do
         const int fl = q.options.flags;
-        pd.quads = q.options.cost == CGS_COST_ZNCC &&
-                   ((fl & CGS_FLAG_QUAD_TAPS) || (!exact_samples(CGS_COST_ZNCC, fl) && !(fl & CGS_FLAG_TEXTURE_TAPS)));
+        pd.quads = pd.route == 1 || (pd.route == 0 && q.options.cost == CGS_COST_ZNCC &&
+                                     ((fl & CGS_FLAG_QUAD_TAPS) ||
+                                      (!exact_samples(CGS_COST_ZNCC, fl) && !(fl & CGS_FLAG_TEXTURE_TAPS))));
         pd.st = staging_layout(q.moving, q.fixed, di.tex_align, di.tex_pitch_align, false, false, pd.quads);
         set_chunks(&pd.p, pd.st, 1, q.fixed.height);
         pd.stage_elems = pd.st.mplane + pd.st.fplane;
@@ -304,6 +402,8 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
     off += 16;
     const size_t tend_off = off;
     off += un * 8;
+    const size_t gnext_off = off;
+    off += 16;
     b->zero_bytes = off - b->zero_off;
     off = align_up(off, 256);
     b->ones_off = off;
@@ -325,18 +425,77 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
     const size_t thdr_off = off;
     off = align_up(off + un * kHeaderBytes, 256);
     const size_t tres_off = off;
-    off = align_up(off + un * sizeof(cgs_argmin), (size_t)di.tex_align);
+    off = align_up(off + un * sizeof(cgs_argmin), 256);
+    // the multi-pair span kernel's pairs: one shared-memory carve for all of them (the largest
+    // tile count, one window stage size), as span_plan sizes it for one pair
+    uint32_t gn = 0;
+    int gtiles = 0;
+    for (int32_t i = 0; i < n; i++)
+        if (pend[i].route == 1) {
+            gn++;
+            gtiles = std::max(gtiles, pend[i].zp.tiles_x * pend[i].zp.tiles_y);
+        }
+    int gcap = 0;
+    if (gn > 0) {
+        const size_t budget = 227 * 1024;
+        const size_t fixed = span_kernel_smem(gplan.G, gplan.NW, gplan.TH, gplan.TX, gtiles, 0);
+        gcap = fixed + (size_t)kMinSpanCap * 32 > budget ? 0 : (int)((budget - fixed) / 32);
+        gcap = std::max(gcap, kMinSpanCap + gplan.TH * 32 * gplan.TX / 4);
+        const size_t gsm = span_kernel_smem(gplan.G, gplan.NW, gplan.TH, gplan.TX, gtiles, gcap);
+        if (fixed + (size_t)kMinSpanCap * 32 > budget || gsm > budget) {
+            for (int32_t i = 0; i < n; i++) pend[i].route = pend[i].route == 1 ? 0 : pend[i].route;
+            gn = 0;  // cannot happen for the sizes span_plan admits; the pairs go to the persistent kernel
+        }
+    }
+    const size_t gpar_off = off;
+    off = align_up(off + gn * sizeof(SearchParams), 256);
+    const size_t gtb_off = off;
+    off = align_up(off + (gn + 1) * 4, 256);
+    const size_t gslot_off = off;
+    off = align_up(off + gn * 4, 256);
+    const size_t gprep_off = off;
+    off = align_up(off + gn * sizeof(SpanPrepArgs), (size_t)di.tex_align);
     std::vector<size_t> stage_off(un);
     for (uint32_t j = 0; j < b->n; j++) {
         stage_off[j] = off;
         off = align_up(off + pend[b->order[j]].st.bytes, (size_t)di.tex_align);
     }
+    for (uint32_t j = 0; j < b->n; j++) {
+        Pending &pd = pend[b->order[j]];
+        if (pd.route != 1) continue;
+        pd.prefix_off = off;
+        const cgs_pair &q = pairs[b->order[j]];
+        off = align_up(off + (size_t)q.fixed.height * (size_t)(q.fixed.width + 1) * sizeof(double2), 256);
+    }
+    off = align_up(off, (size_t)di.tex_align);
+    b->route.assign(un, 0);
+    b->span_pair.resize(un);
+    b->span_off.assign(un, 0);
+    b->span_bytes.assign(un, 0);
+    for (uint32_t j = 0; j < b->n; j++) {
+        const Pending &pd = pend[b->order[j]];
+        b->route[j] = (uint8_t)pd.route;
+        if (pd.route != 2) continue;
+        b->span_pair[j] = pairs[b->order[j]];
+        b->span_off[j] = off;
+        b->span_bytes[j] = pd.span_bytes;
+        off = align_up(off + pd.span_bytes, (size_t)di.tex_align);
+    }
     const size_t total = off;
 
-    cudaError_t e = cudaMalloc(&b->mem, total);
+    // one block from the library's stream-ordered pool: batches created one after another (a
+    // refinement loop) reuse its memory instead of mapping new memory each time
+    cudaMemPool_t pool;
+    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) {
+        release(b);
+        return s;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&b->mem), total, pool, b->cap);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->cap);
     if (e != cudaSuccess) {
         release(b);
-        return cuda_fail(e, "cudaMalloc (batch)");
+        return cuda_fail(e, "cudaMallocFromPoolAsync (batch)");
     }
     b->headers = b->mem + hdr_off;
     b->next_task = reinterpret_cast<unsigned int *>(b->mem + next_off);
@@ -355,6 +514,9 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
     b->params.resize(un);
     b->mi_bins.resize(un);
     b->tex.assign(un, 0);
+    std::vector<SearchParams> gpar;
+    std::vector<uint32_t> gtasks, gslot;
+    std::vector<SpanPrepArgs> gprep;
     for (uint32_t j = 0; j < b->n; j++) {
         const uint32_t i = b->order[j];
         const cgs_pair &q = pairs[i];
@@ -402,24 +564,81 @@ cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_pl
             return cuda_fail(e, "cudaCreateTextureObject");
         }
         p.mov_tex = b->tex[j];
+        if (pd.route == 1) {
+            // as cgs_search sets up its span kernel: quads in the span form with the moving
+            // shift folded in, the fixed rows' prefix sums, tiles and the (common) window stage
+            preps[j].quad_form = 1;
+            double2 *prefix = reinterpret_cast<double2 *>(b->mem + pd.prefix_off);
+            p.fix_prefix = prefix;
+            p.tile_h = pd.zp.TH;
+            p.tiles_x = pd.zp.tiles_x;
+            p.tiles_y = pd.zp.tiles_y;
+            p.win_cap = gcap;
+            p.win_pitch_mod = pd.zp.pitch_mod;
+            const uint32_t per_task = (uint32_t)(pd.zp.G * pd.zp.NW);
+            p.num_tasks = (p.n + per_task - 1) / per_task;
+            gpar.push_back(p);
+            gtasks.push_back(p.num_tasks);
+            gslot.push_back(j);
+            SpanPrepArgs ga;
+            int blocks = 0;
+            span_prep_batch_args(fstage, pd.st.fpitch, q.fixed.width, q.fixed.height, prefix,
+                                 reinterpret_cast<float4 *>(org + pd.st.quad_off), pd.st.qplane, p.shifts, &ga,
+                                 &blocks);
+            gprep.push_back(ga);
+            b->g_prep_blocks = std::max(b->g_prep_blocks, blocks);
+        }
         b->params[j] = p;
         b->mi_bins[j] = pd.mi_bins;
-        b->stage_floats = std::max<int32_t>(b->stage_floats, p.chunk_rows * pd.st.fpitch);
+        if (pd.route == 0) b->stage_floats = std::max<int32_t>(b->stage_floats, p.chunk_rows * pd.st.fpitch);
         b->max_stage_elems = std::max<int64_t>(b->max_stage_elems, pd.stage_elems);
     }
     e = cudaMemcpy(b->d_prep, preps.data(), sizeof(PrepParams) * un, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->last, cudaEventDisableTiming);
+    if (e == cudaSuccess && gn > 0) {
+        // the multi-pair span kernel: its pairs, task prefix, stamp slots, staging arguments, launch shape
+        const std::vector<uint32_t> gtb = prefix(gtasks);
+        b->g_n = gn;
+        b->d_gprep = reinterpret_cast<SpanPrepArgs *>(b->mem + gprep_off);
+        SpanBatchParams &ga = b->g_args;
+        ga.pairs = reinterpret_cast<const SearchParams *>(b->mem + gpar_off);
+        ga.task_begin = reinterpret_cast<const uint32_t *>(b->mem + gtb_off);
+        ga.slot = reinterpret_cast<const uint32_t *>(b->mem + gslot_off);
+        ga.n_pairs = gn;
+        ga.total_tasks = gtb[gn];
+        ga.next_task = reinterpret_cast<unsigned int *>(b->mem + gnext_off);
+        ga.t_start = b->t_start;
+        ga.t_end = b->t_end;
+        ga.tile_h = gplan.TH;
+        ga.tiles = gtiles;
+        ga.cap = gcap;
+        b->g_kfn = kernel_span_zncc_batch(gplan.G, gplan.NW, gplan.TX, gplan.check);
+        b->g_smem = span_kernel_smem(gplan.G, gplan.NW, gplan.TH, gplan.TX, gtiles, gcap);
+        e = cudaMemcpy(b->mem + gpar_off, gpar.data(), sizeof(SearchParams) * gn, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->mem + gtb_off, gtb.data(), 4 * gtb.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->mem + gslot_off, gslot.data(), 4 * gn, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->d_gprep, gprep.data(), sizeof(SpanPrepArgs) * gn, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(b->g_kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->g_smem);
+        int per_sm = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->g_kfn, 16 * 32, b->g_smem);
+        if (e == cudaSuccess && per_sm < 1) e = cudaErrorInvalidConfiguration;
+        b->g_blocks = std::max<uint32_t>(1u, std::min<uint32_t>(ga.total_tasks, (uint32_t)(di.sms * per_sm)));
+    }
     if (e != cudaSuccess) {
         release(b);
         return cuda_fail(e, "batch setup");
     }
-    cgs_batch_plan pl = {2, 16, 0, 0};
+    cgs_batch_plan pl = {4, 16, 0, 0};
     if (plan) {
         pl = *plan;
     } else {
-        // default: 2 points per warp, 16 warps, warp-private MI histograms, unless they do not fit
+        // default: 4 points per warp (MI pairs take 2), 16 warps, warp-private MI histograms;
+        // 2 points per warp, then block-shared histograms, where those do not fit
         Shape sh;
+        if (plan_shape(*b, pl, 0, &sh) != CGS_SUCCESS) pl.points_per_warp = 2;
         if (plan_shape(*b, pl, 0, &sh) != CGS_SUCCESS) pl.block_split = 1;
     }
     if ((s = apply_plan(b, pl)) != CGS_SUCCESS) {
@@ -450,6 +669,12 @@ cgs_status cgs_batch_set_plan(cgs_batch *b, const cgs_batch_plan *plan) {
 cgs_status cgs_batch_get_plan(const cgs_batch *b, cgs_batch_plan *plan) {
     if (!b || !plan) return fail(CGS_ERROR_INVALID_VALUE, "batch or plan is null");
     *plan = b->plan;
+    return CGS_SUCCESS;
+}
+
+cgs_status cgs_batch_kernel_launches(const cgs_batch *b, int32_t *n) {
+    if (!b || !n) return fail(CGS_ERROR_INVALID_VALUE, "batch or output is null");
+    *n = b->kernel_nodes;
     return CGS_SUCCESS;
 }
 

@@ -114,6 +114,12 @@ struct SpanPlan {
     const void *kfn = nullptr;
 };
 bool span_plan(const cgs_image &mov, const cgs_image &fix, const cgs_options &o, SpanPlan *sp);
+// The multi-pair span kernel of batches for a plan (null where not instantiated), and the
+// staging step of many pairs: per pair its arguments and block count, then one launch over all.
+const void *kernel_span_zncc_batch(int G, int NW, int TX, bool check);
+void span_prep_batch_args(const float *fix, int fpitch, int fw, int fh, double2 *prefix, float4 *quads,
+                          int64_t nquads, const float *shifts, SpanPrepArgs *a, int *blocks);
+cudaError_t launch_span_prep_batch(const SpanPrepArgs *args, int n, int blocks, cudaStream_t stream);
 // Span kernel of MI (cgs_span_mi.cuh): 2 points per warp, NW warps, histograms of B <= 32 bins;
 // its shared-memory size and its staging step (the fixed bins times B + 1, int32; the quads'
 // largest slope bound into a header word).
@@ -129,6 +135,21 @@ constexpr int kVerifyMax = CGS_VERIFY_MAX;
 size_t verify_scratch_bytes();
 cgs_status launch_verify(const SearchParams &p, void *hdr, cudaStream_t stream, int sms);
 bool verify_supported(int cost);
+
+// A search in a caller's scratch block (cgs_search.cu): for requests that cgs_search runs on a
+// span kernel (ZNCC or MI on the fast sampling path), the batch runs them with the same launches
+// and results.  span_route_bytes: whether cgs_search runs this pair on a span kernel, the
+// scratch it then needs (staging, span tables, verification header) and the kernel's grid
+// points per task; span_route_enqueue: the search's launches on `stream` with that scratch
+// (tex_align-aligned, `bytes` long).
+struct ExtScratch {
+    char *ptr = nullptr;
+    size_t bytes = 0;
+    bool query = false;
+    uint32_t points_per_task = 0;  // query: the span kernel's grid points per task
+};
+bool span_route_bytes(const cgs_pair &q, size_t *bytes, uint32_t *points_per_task);
+cgs_status span_route_enqueue(const cgs_pair &q, char *scratch, size_t bytes, cudaStream_t stream);
 
 // Plain-load (no texture object) variants at 4 points per warp and 16 warps, for the
 // allocation-free entry point.

@@ -80,6 +80,30 @@ struct SearchParams {
     float2 trig[kMaxTrig];
 };
 
+// The span kernel's staging step of one pair, after prep_kernel (cgs_span.cuh).
+struct SpanPrepArgs {
+    const float *fix;
+    int fpitch, fw, fh;
+    double2 *prefix;
+    int row_blocks;  // blocks [0, row_blocks) write the prefix sums, the others shift the quads
+    float4 *quads;
+    int64_t nquads;
+    const float *shifts;
+};
+
+// Launch parameters of the multi-pair span kernel (cgs_span.cuh).
+struct SpanBatchParams {
+    const SearchParams *pairs;    // [n_pairs], device
+    const uint32_t *task_begin;   // [n_pairs + 1]
+    const uint32_t *slot;         // [n_pairs]: index of the pair's time stamps
+    uint32_t n_pairs, total_tasks;
+    unsigned int *next_task;      // zero at launch
+    unsigned long long *t_start;  // first task start per slot (atomicMin), or null
+    unsigned long long *t_end;    // last task end per slot (atomicMax), or null
+    int32_t tile_h, tiles, cap;
+};
+
+
 // ---------------------------------------------------------------- the map of a grid point
 
 // General projective map of fixed pixel (x, y) to moving coordinates, in the reference's

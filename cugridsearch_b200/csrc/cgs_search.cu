@@ -937,15 +937,25 @@ cgs_status cgs_grid_point(const cgs_grid *g, int64_t index, float out[8]) {
     return CGS_SUCCESS;
 }
 
-cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options *options,
-                      float *costs, cgs_argmin *result, cgs_stream_t stream_) {
-    cudaStream_t stream = (cudaStream_t)stream_;
+}  // extern "C"
+
+namespace cgs {
+
+// The body of cgs_search.  ext = nullptr: scratch from the stream-ordered pool.  ext != nullptr
+// (span searches only, else CGS_ERROR_UNSUPPORTED): the caller's scratch block ext->ptr of
+// ext->bytes bytes holds the staging block, the span tables and the verification header; with
+// ext->query set only the block's size is computed into ext->bytes and nothing is enqueued.
+static cgs_status search_core(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid,
+                              const cgs_options *options, float *costs, cgs_argmin *result, cudaStream_t stream,
+                              ExtScratch *ext) {
     cgs_status s;
     int mi_bins = 32;
     if ((s = check_request(mov, fix, grid, options, &mi_bins)) != CGS_SUCCESS) return s;
-    if (!result) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
+    const bool query = ext && ext->query;
+    if (!result && !query) return fail(CGS_ERROR_INVALID_VALUE, "result is null");
     const cgs_options o = *options;
     const int cost = o.cost;
+    if (is_scanline(cost) && ext) return fail(CGS_ERROR_UNSUPPORTED, "caller scratch: span searches only");
     if (is_scanline(cost)) {
         DeviceInfo dsi;
         if ((s = device_info(&dsi)) != CGS_SUCCESS) return s;
@@ -970,6 +980,7 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     const bool quads = (o.flags & CGS_FLAG_QUAD_TAPS) || (fast_path && !(o.flags & CGS_FLAG_TEXTURE_TAPS)) || span_mi;
     const void *kfn = (span || span_mi) ? sp.kfn : getter(C, pl.G, pl.NW, quads);
     if (!kfn) return fail(CGS_ERROR_UNSUPPORTED, "no kernel for this channel count / tuning");
+    if (ext && !(span || span_mi)) return fail(CGS_ERROR_UNSUPPORTED, "caller scratch: span searches only");
 
     DeviceInfo di;
     if ((s = device_info(&di)) != CGS_SUCCESS) return s;
@@ -978,6 +989,10 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     int64_t n64;
     if ((s = fill_params(mov, fix, grid, o, mi_bins, &p, &n64)) != CGS_SUCCESS) return s;
     if (n64 <= 0) {
+        if (query) {
+            ext->bytes = 0;
+            return CGS_SUCCESS;
+        }
         empty_result_kernel<<<1, 1, 0, stream>>>(result);
         CGS_CUDA(cudaGetLastError(), "empty_result_kernel");
         return CGS_SUCCESS;
@@ -998,17 +1013,31 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
         p.win_pitch_mod = sp.pitch_mod;
     }
 
-    cudaMemPool_t pool;
-    if ((s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
     // the span kernels' tables follow the staging block: the ZNCC kernel's row prefix sums (W_f + 1
     // FP64 pairs per row), the MI kernel's fixed bins (int32, the fixed plane's pitch)
     const size_t prefix_off = (size_t)round_up((int64_t)(st.bytes - (size_t)di.tex_align), 256);
     const size_t prefix_bytes = span      ? (size_t)fix->height * (size_t)(fix->width + 1) * sizeof(double2)
                                 : span_mi ? (size_t)fix->height * (size_t)st.fpitch * sizeof(int32_t)
                                           : 0;
+    const size_t main_bytes = st.bytes + (prefix_bytes ? prefix_bytes + 256 : 0);
+    const bool verify = !(o.flags & CGS_FLAG_NO_VERIFY) && verify_supported(cost);
+    const size_t vbytes = verify ? verify_scratch_bytes() + (costs ? 0 : (size_t)p.n * 4) : 0;
+    const size_t ext_bytes = (size_t)round_up((int64_t)main_bytes, 256) + vbytes;
+    if (query) {
+        ext->bytes = ext_bytes;
+        ext->points_per_task = (uint32_t)(sp.NW * sp.G);
+        return CGS_SUCCESS;
+    }
+    if (ext && ext->bytes < ext_bytes) return fail(CGS_ERROR_INVALID_VALUE, "caller scratch smaller than the search needs");
+    cudaMemPool_t pool = nullptr;
+    if (!ext && (s = get_pool(di.dev, &pool)) != CGS_SUCCESS) return s;
     void *scratch = nullptr;
-    CGS_CUDA(cudaMallocFromPoolAsync(&scratch, st.bytes + (prefix_bytes ? prefix_bytes + 256 : 0), pool, stream),
-             "cudaMallocFromPoolAsync");
+    if (ext) scratch = ext->ptr;
+    else CGS_CUDA(cudaMallocFromPoolAsync(&scratch, main_bytes, pool, stream), "cudaMallocFromPoolAsync");
+    // pool blocks go back to the pool in stream order; a caller's block stays the caller's
+    auto release = [&](void *ptr) {
+        if (!ext && ptr) cudaFreeAsync(ptr, stream);
+    };
     char *sb = staging_origin(scratch, di.tex_align);
     if (span) p.fix_prefix = reinterpret_cast<const double2 *>(sb + prefix_off);
     if (span_mi) {
@@ -1028,14 +1057,16 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     p.result = result;
     // FP64 verification pass after the search: its header, and a cost dump when the caller
     // keeps none (the pass reads the FP32 costs of the band around the minimum)
-    const bool verify = !(o.flags & CGS_FLAG_NO_VERIFY) && verify_supported(cost);
     void *vblock = nullptr;
     if (verify) {
-        const size_t vbytes = verify_scratch_bytes() + (costs ? 0 : (size_t)p.n * 4);
-        cudaError_t ve = cudaMallocFromPoolAsync(&vblock, vbytes, pool, stream);
-        if (ve != cudaSuccess) {
-            cudaFreeAsync(scratch, stream);
-            return cuda_fail(ve, "cudaMallocFromPoolAsync");
+        if (ext) {
+            vblock = ext->ptr + round_up((int64_t)main_bytes, 256);
+        } else {
+            cudaError_t ve = cudaMallocFromPoolAsync(&vblock, vbytes, pool, stream);
+            if (ve != cudaSuccess) {
+                release(scratch);
+                return cuda_fail(ve, "cudaMallocFromPoolAsync");
+            }
         }
         if (!costs) p.costs = reinterpret_cast<float *>(static_cast<char *>(vblock) + verify_scratch_bytes());
     }
@@ -1067,8 +1098,8 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
                                 reinterpret_cast<const float4 *>(sb + st.quad_off), st.qplane,
                                 reinterpret_cast<unsigned int *>(sb + 32), stream);
     if (e != cudaSuccess) {
-        if (vblock) cudaFreeAsync(vblock, stream);
-        cudaFreeAsync(scratch, stream);
+        release(vblock);
+        release(scratch);
         return cuda_fail(e, "prep_kernel");
     }
 
@@ -1081,14 +1112,17 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
     if (e != cudaSuccess || per_sm < 1) {
-        if (vblock) cudaFreeAsync(vblock, stream);
-        cudaFreeAsync(scratch, stream);
+        release(vblock);
+        release(scratch);
         return e != cudaSuccess ? cuda_fail(e, "search kernel setup")
                                 : fail(CGS_ERROR_UNSUPPORTED, "search kernel does not fit on an SM");
     }
     const uint32_t blocks = std::min<uint32_t>(p.num_tasks, (uint32_t)(di.sms * per_sm));
     void *args[] = {&p};
-    {
+    if (ext) {  // the span kernels read tap quads, no texture
+        p.mov_tex = 0;
+        e = cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, smem, stream);
+    } else {
         std::lock_guard<std::mutex> lock(g_tex_mu);
         TexEntry *te = nullptr;
         s = texture_for(di.dev, mstage, mov->width + 1, C * (mov->height + 1), (size_t)st.mpitch * 4, &te);
@@ -1102,11 +1136,41 @@ cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid
         e = cudaMemsetAsync(vblock, 0, 8, stream);  // band count and CTA ticket
         if (e == cudaSuccess) s = launch_verify(p, vblock, stream, di.sms);
     }
-    if (vblock) cudaFreeAsync(vblock, stream);
-    cudaFreeAsync(scratch, stream);
+    release(vblock);
+    release(scratch);
     if (s != CGS_SUCCESS) return s;
     if (e != cudaSuccess) return cuda_fail(e, "search kernel launch");
     return CGS_SUCCESS;
+}
+
+bool span_route_bytes(const cgs_pair &q, size_t *bytes, uint32_t *points_per_task) {
+    static float dummy;  // stands for a caller's cost dump: only its presence matters here
+    ExtScratch x;
+    x.query = true;
+    const std::string keep = g_last_error;
+    const cgs_status s = search_core(&q.moving, &q.fixed, &q.grid, &q.options, q.costs ? &dummy : nullptr, nullptr,
+                                     nullptr, &x);
+    g_last_error = keep;  // "not a span search" is an answer here, not an error
+    if (s != CGS_SUCCESS || x.bytes == 0) return false;
+    *bytes = x.bytes;
+    *points_per_task = x.points_per_task;
+    return true;
+}
+
+cgs_status span_route_enqueue(const cgs_pair &q, char *scratch, size_t bytes, cudaStream_t stream) {
+    ExtScratch x;
+    x.ptr = scratch;
+    x.bytes = bytes;
+    return search_core(&q.moving, &q.fixed, &q.grid, &q.options, q.costs, q.result, stream, &x);
+}
+
+}  // namespace cgs
+
+extern "C" {
+
+cgs_status cgs_search(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid, const cgs_options *options,
+                      float *costs, cgs_argmin *result, cgs_stream_t stream_) {
+    return search_core(mov, fix, grid, options, costs, result, (cudaStream_t)stream_, nullptr);
 }
 
 cgs_status cgs_search_sync(const cgs_image *mov, const cgs_image *fix, const cgs_grid *grid,

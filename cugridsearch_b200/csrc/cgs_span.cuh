@@ -746,25 +746,24 @@ __global__ void __launch_bounds__(NW * 32, 1) span_kernel(const __grid_constant_
     }
 }
 
-// The span kernel's staging step, after prep_kernel: blocks [0, row_blocks) write the FP64
-// prefix sums of each staged fixed row, prefix[y (W + 1) + x] = {sum f, sum f^2} of pixels
-// 0 .. x - 1 of row y (channel 0; one warp per row, a warp scan per 32 pixels carried in order,
-// so the sums are the same in every run); the other blocks subtract the moving image's shift
-// from every quad's constant term, so that the sweep's bilinear values are shifted already.
-static __global__ void __launch_bounds__(256)
-span_prep_kernel(const float *__restrict__ fix, int fpitch, int fw, int fh, double2 *__restrict__ prefix,
-                 int row_blocks, float4 *__restrict__ quads, int64_t nquads, const float *__restrict__ shifts) {
-    if ((int)blockIdx.x >= row_blocks) {
-        const float ms = shifts[1];
-        const int64_t nthr = (int64_t)(gridDim.x - row_blocks) * blockDim.x;
-        for (int64_t i = (int64_t)(blockIdx.x - row_blocks) * blockDim.x + threadIdx.x; i < nquads; i += nthr)
-            quads[i].x -= ms;
+// Blocks [0, row_blocks) write the FP64 prefix sums of each staged fixed row, prefix[y (W + 1) +
+// x] = {sum f, sum f^2} of pixels 0 .. x - 1 of row y (channel 0; one warp per row, a warp scan
+// per 32 pixels carried in order, so the sums are the same in every run); the other blocks of
+// the `nblocks` subtract the moving image's shift from every quad's constant term, so that the
+// sweep's bilinear values are shifted already.
+__device__ __forceinline__ void span_prep_body(const SpanPrepArgs &a, int block, int nblocks) {
+    if (block >= a.row_blocks) {
+        const float ms = a.shifts[1];
+        const int64_t nthr = (int64_t)(nblocks - a.row_blocks) * blockDim.x;
+        for (int64_t i = (int64_t)(block - a.row_blocks) * blockDim.x + threadIdx.x; i < a.nquads; i += nthr)
+            a.quads[i].x -= ms;
         return;
     }
-    const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (row >= fh) return;
-    const float *src = fix + (int64_t)row * fpitch;
-    double2 *dst = prefix + (int64_t)row * (fw + 1);
+    const int row = (int)((block * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (row >= a.fh) return;
+    const int fw = a.fw;
+    const float *src = a.fix + (int64_t)row * a.fpitch;
+    double2 *dst = a.prefix + (int64_t)row * (fw + 1);
     if (lane == 0) dst[0] = make_double2(0.0, 0.0);
     double c1 = 0.0, c2 = 0.0;
     for (int x0 = 0; x0 < fw; x0 += 32) {
@@ -782,6 +781,74 @@ span_prep_kernel(const float *__restrict__ fix, int fpitch, int fw, int fh, doub
         if (x < fw) dst[x + 1] = make_double2(c1 + v, c2 + v2);
         c1 += __shfl_sync(0xffffffffu, v, 31);
         c2 += __shfl_sync(0xffffffffu, v2, 31);
+    }
+}
+
+static __global__ void __launch_bounds__(256) span_prep_kernel(const SpanPrepArgs a) {
+    span_prep_body(a, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// The staging step of many pairs at once: pair blockIdx.y, its blocks blockIdx.x (gridDim.x
+// exceeds every pair's row_blocks).
+static __global__ void __launch_bounds__(256) span_prep_batch_kernel(const SpanPrepArgs *__restrict__ args) {
+    span_prep_body(args[blockIdx.y], (int)blockIdx.x, (int)gridDim.x);
+}
+
+// ---------------------------------------------------------------- the multi-pair span kernel
+//
+// Batches: the tasks of many ZNCC pairs (each with its own staged planes, prefix sums, tiles
+// and grid) from one counter, so that pairs too small to fill the GPU alone share it.  A
+// task's pair is found in the prefix of task counts; its parameters are read from global
+// memory.  Shared memory is carved once for the largest tile count of the pairs and one window
+// stage size (`cap`) for all of them; each pair's results are those of span_kernel on that pair.
+template <int G, int NW, int TX, bool CHECK>
+__global__ void __launch_bounds__(NW * 32, 1) span_batch_kernel(const __grid_constant__ SpanBatchParams b) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const SpanSmem ss = carve_span<G, NW>(smem, b.tile_h, TX, b.tiles, b.cap);
+    // the task word sits in the carve's head, after the flags (no static shared memory: the
+    // dynamic carve may take all 227 KB)
+    volatile uint32_t &s_task = *reinterpret_cast<volatile uint32_t *>(ss.bounds_flag + 1);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWinStages; s++) mbar_init(&ss.bars[s], 1);
+        fence_mbar_init();
+        *ss.abort_flag = 0;
+        *ss.bounds_flag = 0;
+    }
+    uint32_t wit = 0;
+    for (;;) {
+        __syncthreads();  // the previous task is done with s_task
+        if (threadIdx.x == 0) s_task = atomicAdd(b.next_task, 1u);
+        __syncthreads();
+        const uint32_t t = s_task;
+        if (t >= b.total_tasks) return;
+        uint32_t lo = 0, hi = b.n_pairs;  // task_begin[lo] <= t < task_begin[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(b.task_begin + mid) <= t) lo = mid;
+            else hi = mid;
+        }
+        const SearchParams &p = b.pairs[lo];
+        const uint32_t slot = __ldg(b.slot + lo);
+        if (threadIdx.x == 0 && b.t_start) atomicMin(b.t_start + slot, (unsigned long long)global_ns());
+        if (!run_span_task<G, NW, TX, CHECK>(p, t - __ldg(b.task_begin + lo), ss, wit)) {
+            if (threadIdx.x == 0) {
+                // retire this task and every task not yet taken, with the timeout status
+                retire_tasks(p, ~0ull, 1u, true);
+                for (;;) {
+                    const uint32_t u = atomicAdd(b.next_task, 1u);
+                    if (u >= b.total_tasks) break;
+                    uint32_t l2 = 0, h2 = b.n_pairs;
+                    while (h2 - l2 > 1) {
+                        const uint32_t mid = (l2 + h2) >> 1;
+                        if (__ldg(b.task_begin + mid) <= u) l2 = mid;
+                        else h2 = mid;
+                    }
+                    retire_tasks(b.pairs[l2], ~0ull, 1u, true);
+                }
+            }
+            return;
+        }
+        if (threadIdx.x == 0 && b.t_end) atomicMax(b.t_end + slot, (unsigned long long)global_ns());
     }
 }
 

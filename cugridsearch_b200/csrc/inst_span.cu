@@ -1,6 +1,7 @@
 // Span-kernel instantiations (zero-mean NCC, one channel), 16 warps per CTA: 4 points per warp
 // with tiles of 64, 128 or 256 columns, 2 points per warp with 128 or 256; plain and self-checking;
-// and the fixed rows' prefix sums.
+// the multi-pair kernel of batches (4 points per warp, tiles of 256 columns); and the fixed rows'
+// prefix sums.
 #include <algorithm>
 
 #include "cgs_internal.h"
@@ -34,12 +35,29 @@ size_t span_kernel_smem(int G, int NW, int TH, int TX, int tiles, int cap) {
 
 int64_t span_max_quads() { return kSpanMaxQuads; }
 
+static int span_prep_row_blocks(int fh) { return (int)(((int64_t)fh * 32 + 255) / 256); }
+static int span_prep_quad_blocks(int64_t nquads) { return (int)std::min<int64_t>((nquads + 255) / 256, 1024); }
+
 cudaError_t launch_span_prep(const float *fix, int fpitch, int fw, int fh, double2 *prefix, float4 *quads,
                              int64_t nquads, const float *shifts, cudaStream_t stream) {
-    const int row_blocks = (int)(((int64_t)fh * 32 + 255) / 256);
-    const int quad_blocks = (int)std::min<int64_t>((nquads + 255) / 256, 1024);
-    span_prep_kernel<<<row_blocks + quad_blocks, 256, 0, stream>>>(fix, fpitch, fw, fh, prefix, row_blocks, quads,
-                                                                   nquads, shifts);
+    const SpanPrepArgs a{fix, fpitch, fw, fh, prefix, span_prep_row_blocks(fh), quads, nquads, shifts};
+    span_prep_kernel<<<a.row_blocks + span_prep_quad_blocks(nquads), 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+const void *kernel_span_zncc_batch(int G, int NW, int TX, bool check) {
+    if (G == 4 && NW == 16 && TX == 8 && !check) return (const void *)span_batch_kernel<4, 16, 8, false>;
+    return nullptr;
+}
+
+void span_prep_batch_args(const float *fix, int fpitch, int fw, int fh, double2 *prefix, float4 *quads,
+                          int64_t nquads, const float *shifts, SpanPrepArgs *a, int *blocks) {
+    *a = SpanPrepArgs{fix, fpitch, fw, fh, prefix, span_prep_row_blocks(fh), quads, nquads, shifts};
+    *blocks = a->row_blocks + span_prep_quad_blocks(nquads);
+}
+
+cudaError_t launch_span_prep_batch(const SpanPrepArgs *args, int n, int blocks, cudaStream_t stream) {
+    span_prep_batch_kernel<<<dim3(blocks, n), 256, 0, stream>>>(args);
     return cudaGetLastError();
 }
 

@@ -320,8 +320,11 @@ typedef struct cgs_batch cgs_batch; /* opaque handle */
 /* Creates a batch: validates every pair, lays out device scratch for all of them (one
  * allocation, held until cgs_batch_destroy), orders the pairs by estimated work (cheapest
  * first) and records one CUDA graph -- clear scratch, stage every pair, the persistent batch
- * kernel -- for the plan (NULL: 2 points per warp, 16 warps, warp-private histograms, or
- * block-shared ones where those do not fit).  The images, dumps and results are bound to the
+ * kernel over the pairs' tasks, then, pair after pair, the launches of cgs_search for the ZNCC
+ * and MI pairs that cgs_search runs on its span kernels (fast sampling, no per-sample flag;
+ * their results are cgs_search's bit for bit, FP64 verification included) -- for the plan
+ * (NULL: 4 points per warp, 16 warps, warp-private histograms; 2 points per warp, then
+ * block-shared histograms, where those do not fit).  The images, dumps and results are bound to the
  * handle: update image CONTENTS in place between launches.  Errors name the failing pair. */
 cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_plan *plan, cgs_batch **batch);
 
@@ -340,8 +343,13 @@ cgs_status cgs_batch_autotune(cgs_batch *batch, int32_t sample_points, cgs_tune_
                               int32_t *n_entries, cgs_batch_plan *best);
 
 /* Device time stamps (%globaltimer, ns) of the last launch, per pair in the caller's order: the
- * start of the pair's first task and the end of its last.  Waits for the launch. */
+ * start of the pair's first task and the end of its last (pairs searched by span kernels: the
+ * start and end of their own launches).  Waits for the launch. */
 cgs_status cgs_batch_pair_times(cgs_batch *batch, uint64_t *start_ns, uint64_t *end_ns);
+
+/* Kernel launches of one cgs_batch_launch (the kernel nodes of the recorded graph).  No
+ * counterpart in the reference. */
+cgs_status cgs_batch_kernel_launches(const cgs_batch *batch, int32_t *n);
 
 /* Releases the handle's graph, textures and device memory (waits for its last launch). */
 cgs_status cgs_batch_destroy(cgs_batch *batch);

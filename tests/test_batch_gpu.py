@@ -1,12 +1,18 @@
 """The batched search (cgs_batch_* / cgs_search_batched) on the GPU.
 
-A batch evaluates many pairs of uneven sizes, each with its own grid and cost, in one
-persistent launch.  Its per-pair results are checked against cgs_search on the same pair
-(itself checked against the oracle in test_gpu_parity.py):
+A batch evaluates many pairs of uneven sizes, each with its own grid and cost: the persistent
+kernel over the per-sample pairs' tasks, the multi-pair span kernel over the ZNCC pairs that
+cgs_search runs on its span kernel, and cgs_search's own launches for MI pairs whose grids fill
+the GPU (CGS_BATCH_SPAN_TASKS_PER_SM tasks per SM, default 4; the small MI grids here stay in the
+persistent kernel unless a test sets it to 0).  Its per-pair results are checked against
+cgs_search on the same pair (itself checked against the oracle in test_gpu_parity.py):
   * block_split = 0: costs bit-identical for every points-per-warp / warps-per-block plan
-    (each point's pixels are summed in the same order whatever the plan);
+    (each point's pixels are summed in the same order whatever the plan; ZNCC pairs as
+    cgs_search's span kernel, MI pairs as its per-sample and span kernels, which agree bit for bit);
   * block_split = 1: MI costs bit-identical (exact counts, same final sum), the others
     within the FP32 summation-order tolerance; argmins equal where separated;
+  * ZNCC and MI pairs with per-sample decisions run in the persistent kernel, bit-identical to
+    cgs_search with the same flag;
 and the pairs' costs against the FP64 oracle directly on a small batch.  Also: graph replay
 after the images change in place, the autotuner, per-pair time stamps, the one-shot entry.
 """
@@ -47,23 +53,22 @@ def _make(cuda, specs, seed=7):
     return items
 
 
-def _single(cuda, items):
-    """cgs_search per pair: (costs, argmin) on the host.  The batch runs every cost on the per-sample
-    decision kernel, so ZNCC pairs are compared with that kernel (CGS_FLAG_PER_SAMPLE_DECISIONS);
-    test_batch_zncc_agrees_with_span_kernel covers the single search's default ZNCC kernel."""
+def _single(cuda, items, per_sample=False):
+    """cgs_search per pair: (costs, argmin) on the host, with the batch pairs' flags."""
     import torch
     import cugridsearch_b200 as cgs
     out = []
     for it in items:
         c = torch.empty(it["grid"].numElements(), dtype=torch.float32, device=cuda)
-        r = cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c, per_sample_decisions=True)
+        r = cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c, per_sample_decisions=per_sample)
         out.append((c.cpu().numpy(), r))
     return out
 
 
-def _batch_pairs(items):
+def _batch_pairs(items, per_sample=False):
     import cugridsearch_b200 as cgs
-    return [cgs.BatchPair(it["cost"], it["mov"], it["fix"], it["grid"], it["result"], it["costs"]) for it in items]
+    return [cgs.BatchPair(it["cost"], it["mov"], it["fix"], it["grid"], it["result"], it["costs"],
+                          per_sample_decisions=per_sample) for it in items]
 
 
 def _read(items):
@@ -173,7 +178,7 @@ def test_batch_graph_replay_follows_image_contents(cuda, items, reference):
             torch.cuda.synchronize()
             c_new = it["costs"].cpu().numpy()
             c_chk = torch.empty_like(it["costs"])
-            cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c_chk, per_sample_decisions=True)
+            cgs.search(it["cost"], it["mov"], it["fix"], it["grid"], costs=c_chk)
             np.testing.assert_array_equal(c_new.view(np.uint32), c_chk.cpu().numpy().view(np.uint32))
             assert not np.array_equal(c_new, reference[1][0])
         finally:
@@ -216,20 +221,67 @@ def test_search_batched_one_shot(cuda, items, reference):
         assert r.index == r_ref.index
 
 
-def test_batch_zncc_agrees_with_span_kernel(cuda, items, lib):
-    """ZNCC pairs of a batch (per-sample decision kernel) against cgs_search's default ZNCC kernel
-    (the span kernel): same finite pattern, costs within the FP32 summation tolerance."""
+@pytest.mark.parametrize("g,w,bs", [(2, 16, 0), (4, 8, 0), (1, 16, 1)])
+def test_batch_per_sample_pairs_in_the_persistent_kernel(cuda, items, g, w, bs):
+    """With per-sample decisions the ZNCC and MI pairs run in the persistent kernel too: costs
+    bit-identical to cgs_search with the same flag (block_split = 1: MI exactly, ZNCC within the
+    summation-order tolerance)."""
     import torch
     import cugridsearch_b200 as cgs
+    ref = _single(cuda, items, per_sample=True)
+    try:
+        batch = cgs.Batch(_batch_pairs(items, per_sample=True), cgs.BatchPlan(g, w, bs))
+    except cgs.CgsError as e:
+        assert e.status == 2, e
+        pytest.skip(str(e))
+    with batch:
+        batch.launch()
+        torch.cuda.synchronize()
+        got = _read(items)
+        t0, t1 = batch.pair_times()
+    for (c_ref, r_ref), (c, r), it in zip(ref, got, items):
+        if bs == 0 or it["cost"] == "MI":
+            np.testing.assert_array_equal(c.view(np.uint32), c_ref.view(np.uint32), err_msg=it["cost"])
+            assert r.index == r_ref.index
+        else:
+            fin = np.isfinite(c_ref)
+            assert np.array_equal(np.isfinite(c), fin)
+            scale = {"SQD_REF": 1e-3}.get(it["cost"], 1.0)
+            assert np.all(np.abs(c[fin] - c_ref[fin]) <= 2e-5 * np.maximum(np.abs(c_ref[fin]), scale)), it["cost"]
+        assert r.status == 0
+    assert np.all(t0 > 0) and np.all(t1 >= t0)
+
+
+def test_batch_span_pairs_follow_cgs_search(cuda, items, reference, monkeypatch):
+    """The ZNCC pairs share one multi-pair span launch and get cgs_search's span-kernel costs bit
+    for bit; with every span-eligible pair routed (CGS_BATCH_SPAN_TASKS_PER_SM=0) the MI pairs
+    are searched by cgs_search's own launches, FP64 verification included.  The graph holds
+    staging, the span staging step, the persistent kernel and the multi-pair span kernel, plus
+    the routed pairs' launches."""
+    import torch
+    import cugridsearch_b200 as cgs
+    with cgs.Batch(_batch_pairs(items)) as b0:
+        assert b0.kernel_launches == 4
+        b0.launch()
+        torch.cuda.synchronize()
+        got = _read(items)
+        t0, t1 = b0.pair_times()
+    for (c_ref, r_ref), (c, r), it in zip(reference, got, items):
+        np.testing.assert_array_equal(c.view(np.uint32), c_ref.view(np.uint32), err_msg=it["cost"])
+        assert r.index == r_ref.index and r.status == 0
+    assert np.all(t0 > 0) and np.all(t1 >= t0)
+    monkeypatch.setenv("CGS_BATCH_SPAN_TASKS_PER_SM", "0")
     with cgs.Batch(_batch_pairs(items)) as b:
+        assert b.kernel_launches > 4 + 4 * sum(it["cost"] == "MI" for it in items)
         b.launch()
         torch.cuda.synchronize()
-    for it, (c, r) in zip(items, _read(items)):
-        if it["cost"] != "ZNCC":
+        got = _read(items)
+        t0, t1 = b.pair_times()
+    for (c_ref, r_ref), (c, r), it in zip(reference, got, items):
+        np.testing.assert_array_equal(c.view(np.uint32), c_ref.view(np.uint32), err_msg=it["cost"])
+        if it["cost"] != "MI":
             continue
-        cs = torch.empty(it["grid"].numElements(), dtype=torch.float32, device=cuda)
-        cgs.search("ZNCC", it["mov"], it["fix"], it["grid"], costs=cs)
-        s = cs.cpu().numpy()
-        fin = np.isfinite(s)
-        np.testing.assert_array_equal(np.isfinite(c), fin)
-        assert np.max(np.abs(c[fin] - s[fin]) / np.maximum(np.abs(s[fin]), 1.0)) <= 1e-5
+        assert (r.index, r.valid, r.status, r.verified, r.index_fp64) == \
+            (r_ref.index, r_ref.valid, r_ref.status, r_ref.verified, r_ref.index_fp64)
+        assert r.cost_fp64 == r_ref.cost_fp64 and r.err_fp64 == r_ref.err_fp64
+    assert np.all(t0 > 0) and np.all(t1 >= t0)
