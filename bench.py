@@ -43,7 +43,8 @@ WORKLOADS = {
     "mi": "mi-single-pair 512x512 u8 (gamma-remapped moving), MI 32x32 bins, 5^8 = 390,625 grid points",
     "sad": "sad-small 64x64 f32, SAD over the overlap (averageAbsoluteDifference), 4^8 = 65,536 grid points",
     "batch": "batched-uneven-pairs: 64 pairs, square f32 128-1024 px (log-uniform), costs SAD / ZNCC / MI-32 "
-             "in turn, own ranges, 4-6 values per parameter; one persistent launch replayed from a CUDA graph",
+             "in turn, own ranges, 4-6 values per parameter; one recorded launch sequence (persistent kernel, "
+             "multi-pair span kernel, MI span searches) replayed from a CUDA graph",
 }
 WORKLOAD = WORKLOADS["ncc"]
 METRIC = "homography evals/s"
@@ -449,7 +450,7 @@ def main():
                     help="tap source of the fast path (auto: the library's choice)")
     ap.add_argument("--workload", default="ncc", choices=["ncc", "mi", "sad", "batch"],
                     help="ncc: the headline 256^2 ZNCC pair; mi: 512^2 u8 MI pair; sad: 64^2 SAD pair; "
-                         "batch: 64 uneven pairs in one persistent launch")
+                         "batch: 64 uneven pairs in one batch launch")
     ap.add_argument("--autotune", type=int, default=0,
                     help="batch: autotune the plan on this many points per pair first (0 = default plan)")
     ap.add_argument("--pairs", type=int, default=64, help="batch: number of pairs")

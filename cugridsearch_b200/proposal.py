@@ -184,7 +184,7 @@ def full_grid(side: int = 256, values: int = 6):
 
 
 def _batch_search(cost, fixed, moving, grids, device, dump=None):
-    """One persistent launch over pairs i with grid grids[i]: (params (n, 8), costs (n,),
+    """One batch launch over pairs i with grid grids[i]: (params (n, 8), costs (n,),
     valid (n,), points evaluated).  dump: indices of the pairs whose whole cost arrays are
     wanted; they are then returned as a fifth element (dict index -> numpy array)."""
     import torch
@@ -208,7 +208,7 @@ def _batch_search(cost, fixed, moving, grids, device, dump=None):
 
 def grid_argmins(fixed, moving, grid, cost: str = "ZNCC", chunk: int = 256):
     """The grid-search argmin of every pair (the full grid's answer), in chunks of pairs per
-    persistent launch.  fixed, moving: CUDA float32 (n, side, side).  Returns (params, costs)."""
+    batch launch.  fixed, moving: CUDA float32 (n, side, side).  Returns (params, costs)."""
     n = int(fixed.shape[0])
     ps, cs = [], []
     for i in range(0, n, chunk):
@@ -233,14 +233,14 @@ def serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", min_values:
     """The learned-proposal path for a batch of pairs.
 
     1. The network proposes a window of the full grid per pair (cgs_proposal_window).  One
-       persistent launch searches every pair's window and a coarse probe of the full grid
+       batch launch searches every pair's window and a coarse probe of the full grid
        (full-grid points, so its best bounds the full grid's best from above).
     2. With starts = k > 1, k - 1 more walkers per pair start from min_values-wide windows
        centred on the probe's k - 1 best points.
     3. A walker whose window's best lies strictly inside the window on every axis (or on a
        window edge that is the grid's edge) stops there: a certified local minimum of the grid.
        A best on an inner window edge moves the window to centre on it, at most `walks` times.
-       Every pass over the pending walkers of all pairs is one persistent launch.
+       Every pass over the pending walkers of all pairs is one batch launch.
     4. A pair's answer is the best certified point (or the probe's best, if lower); a pair
        without any certified point is searched on the full grid (the fallback)."""
     n = int(fixed.shape[0])
@@ -326,7 +326,7 @@ def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", valu
 
     1. The network's centre and radii (grid-range units) give each pair a local grid of `values`
        values per axis over centre +- spread x radius (at least min_half of the range, clipped
-       to the full grid's range).  One persistent launch searches every pair's local grid and a
+       to the full grid's range).  One batch launch searches every pair's local grid and a
        coarse probe of the full grid (`probe_values` full-grid values per axis).
     2. Coarse to fine, as the reference's driver loop (src/gpu/cudaGridSearch_main_mi.cu:
        312-363): each further launch re-centres every pair's grid on its best point with half the
