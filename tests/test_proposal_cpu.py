@@ -189,3 +189,55 @@ def test_serve_logic_with_oracle_search(lib, monkeypatch):
     # more starts (the probe's best points) still return the argmins
     r3 = P.serve(Net(off), fixed, moving, full, min_values=3, max_values=3, walks=3, starts=3)
     np.testing.assert_allclose(r3.costs, tcost, rtol=1e-6, atol=1e-7)
+
+
+def test_refine_serve_logic_with_oracle_search(lib, monkeypatch):
+    """The refinement serving (local grids around the proposal, coarse to fine levels, edge walks,
+    coarse probe, fallback) with the searches done by the oracle: started at the full grid's
+    argmin it never returns a worse cost; every level is one batch search over the pairs still
+    refining; a proposal far from the argmin with a tiny radius ends above the probe's best and
+    falls back to the full grid's answer; the points evaluated are counted."""
+    from cugridsearch_b200 import proposal as P
+    from cugridsearch_b200 import synthetic as S
+    calls = []
+
+    def counted(cost, fixed, moving, grids, device, dump=None):
+        calls.append(len(grids))
+        return _oracle_batch_search(cost, fixed, moving, grids, device, dump)
+
+    monkeypatch.setattr(P, "_batch_search", counted)
+    pairs = [S.small_pair(600 + i, size=16, count=4, cost="ZNCC") for i in range(3)]
+    fixed = torch.from_numpy(np.stack([p.fixed[:, :, 0] for p in pairs]))
+    moving = torch.from_numpy(np.stack([p.moving[:, :, 0] for p in pairs]))
+    from cugridsearch_b200 import CudaGrid
+    full = CudaGrid.from_ranges(*pairs[0].grid_args())
+    truth, tcost, _, _ = _oracle_batch_search("ZNCC", fixed, moving, [full] * 3, None)
+    assert np.all(np.isfinite(tcost))
+
+    class Net:
+        def __init__(self, out):
+            self.out = out
+
+        def forward(self, f, m):
+            return torch.from_numpy(self.out)
+
+    zero = np.zeros((3, 16), np.float32)
+    # started at the argmin: the first local grid holds it, so no answer costs more
+    calls.clear()
+    r = P.refine_serve(Net(zero), fixed, moving, full, values=3, levels=2, walks=0, start=truth)
+    assert np.all(r.costs <= tcost + 1e-7) and not r.fallback.any()
+    assert calls[0] == 6  # three local grids and three coarse probes in one search
+    assert len(calls) <= 3 and all(c <= 3 for c in calls[1:])  # then one search per level
+    # the counted points are the grids actually searched
+    assert r.points == 3 * 3 ** 8 + 3 * 3 ** 8 + sum(calls[1:]) * 3 ** 8
+    # far off (a corner of the range, the smallest radius): the refined cost is above the probe's
+    # best for at least one pair, which then takes the full grid's answer
+    lo, hi = full.matrix()[0], full.matrix()[1]
+    far = np.concatenate([np.full((3, 8), 0.999), np.full((3, 8), -12.0)], 1).astype(np.float32)
+    calls.clear()
+    r2 = P.refine_serve(Net(far), fixed, moving, full, values=3, levels=1, walks=0, min_half=1e-4)
+    assert r2.fallback.any()
+    fb = r2.fallback
+    np.testing.assert_allclose(r2.costs[fb], tcost[fb], rtol=1e-6, atol=1e-7)
+    assert calls[-1] == int(fb.sum())  # the fallback searches the full grid of those pairs only
+    assert np.all(r2.params >= lo - 1e-6) and np.all(r2.params <= hi + 1e-6)
