@@ -285,3 +285,22 @@ def test_batch_span_pairs_follow_cgs_search(cuda, items, reference, monkeypatch)
             (r_ref.index, r_ref.valid, r_ref.status, r_ref.verified, r_ref.index_fp64)
         assert r.cost_fp64 == r_ref.cost_fp64 and r.err_fp64 == r_ref.err_fp64
     assert np.all(t0 > 0) and np.all(t1 >= t0)
+
+
+def test_batch_zncc_group_of_mixed_sizes(cuda, lib):
+    """ZNCC pairs of different sizes share one multi-pair span launch (one shared-memory carve for
+    the largest tile count, one window stage for all): each pair's costs and argmin equal
+    cgs_search's bit for bit."""
+    import torch
+    import cugridsearch_b200 as cgs
+    specs = [("ZNCC", 300, 280, 2), ("ZNCC", 64, 60, 3), ("ZNCC", 200, 210, 2), ("ZNCC", 130, 130, 2)]
+    its = _make(cuda, specs, seed=211)
+    ref = _single(cuda, its)
+    with cgs.Batch(_batch_pairs(its)) as b:
+        assert b.kernel_launches == 3  # staging, span staging, the multi-pair span kernel
+        b.launch()
+        torch.cuda.synchronize()
+        got = _read(its)
+    for (c_ref, r_ref), (c, r), it in zip(ref, got, its):
+        np.testing.assert_array_equal(c.view(np.uint32), c_ref.view(np.uint32))
+        assert r.index == r_ref.index and r.status == 0 and r.valid == r_ref.valid
