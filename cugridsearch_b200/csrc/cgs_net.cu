@@ -974,12 +974,33 @@ __global__ void fc_bwd_weight_kernel(const float *__restrict__ dout, const float
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nout * (nin + 1)) return;
     const int j = i / (nin + 1), k = i - j * (nin + 1);
+    // summed over the batch in order; the loads of 8 batch rows are issued before their 8
+    // multiply-adds, so the loop waits on memory once per 8 rows instead of once per row
     float s = 0.0f;
     if (k < nin) {
-        for (int b = 0; b < n; b++) s = fmaf(dout[(int64_t)b * nout + j], in[(int64_t)b * nin + k], s);
+        int b = 0;
+        for (; b + 8 <= n; b += 8) {
+            float u[8], v[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                u[t] = dout[(int64_t)(b + t) * nout + j];
+                v[t] = in[(int64_t)(b + t) * nin + k];
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++) s = fmaf(u[t], v[t], s);
+        }
+        for (; b < n; b++) s = fmaf(dout[(int64_t)b * nout + j], in[(int64_t)b * nin + k], s);
         dw[(int64_t)j * nin + k] = s;
     } else {
-        for (int b = 0; b < n; b++) s += dout[(int64_t)b * nout + j];
+        int b = 0;
+        for (; b + 8 <= n; b += 8) {
+            float u[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) u[t] = dout[(int64_t)(b + t) * nout + j];
+#pragma unroll
+            for (int t = 0; t < 8; t++) s += u[t];
+        }
+        for (; b < n; b++) s += dout[(int64_t)b * nout + j];
         db[j] = s;
     }
 }
