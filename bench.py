@@ -237,8 +237,9 @@ def reference_arm(args):
 
 def measure_batch(dev, rank: int, world: int, n_pairs: int, steps: int, warmup: int, autotune: int = 0) -> dict:
     """The batched uneven pairs on one GPU: pairs/s of one batch launch (graph replay of the
-    persistent kernel and the span-kernel searches, CUDA events), per-pair completion latency p50/p99 from the kernel's time stamps, and the end-to-end
-    rate with the images copied in from pinned host memory and the results copied out every step."""
+    persistent kernel and the span-kernel searches, CUDA events), per-pair completion latency
+    p50/p99 from the kernels' time stamps, and the end-to-end rate with the images copied in from
+    pinned host memory and the results copied out every step."""
     import torch
     import cugridsearch_b200 as cgs
     from cugridsearch_b200 import synthetic as S

@@ -5,7 +5,7 @@ is worse than a coarse probe of the full grid.
 
 The reference has no learned component; its drivers search the full grid, optionally
 shrinking the range around the argmin level by level (src/gpu/cudaGridSearch_main_mi.cu:
-312-363).  Here the full grid stays the judge: labels are the full grid's own argmins, and a
+312-363).  Here the full grid stays the arbiter: labels are the full grid's own argmins, and a
 pair whose proposal cannot beat the coarse probe is searched in full.
 
 Parameters are exchanged in grid-range units: ``u = 2 (p - start) / (end - start) - 1`` per
@@ -458,12 +458,12 @@ def train(net: ProposalNet, fixed, moving, labels_u, epochs: int, batch: int = 2
 def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, label_side: int = 128,
                min_values: int = 3, max_values: int = 5, batch: int = 256, checkpoint: str | None = None,
                variants=None, init: str | None = None, labels: str = "grid", lr: float = 1e-3,
-               judge: str | None = None, mode: str = "lattice", scene: bool = False, log=print) -> dict:
+               full_grid_cache: str | None = None, mode: str = "lattice", scene: bool = False, log=print) -> dict:
     """The learned-proposal configuration end to end on the current GPU: generate training pairs
     (256 px), label them -- labels="grid": the full 6^8 ZNCC grid's argmin on the pairs box-averaged
     to label_side; labels="truth": the generator's ground-truth parameters, no search -- train, then
-    on held-out 256 px pairs compare the served proposal path with the full grid (the judge):
-    corner error, cost gap, fallback rate and pairs/s of both (CUDA events).  judge: an .npz
+    on held-out 256 px pairs compare the served proposal path with the full grid (the arbiter):
+    corner error, cost gap, fallback rate and pairs/s of both (CUDA events).  full_grid_cache: an .npz
     holding the full grid's argmins of the same held-out pairs (written here when absent); with
     it, the full grid is timed on the first 64 pairs only."""
     import json
@@ -516,13 +516,13 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
         ckpt = os.path.join(out_dir, "proposal_net.npz")
         net.save(ckpt)
         del F, M
-    # evaluation at 256 px: the full grid (the judge) once, then each serving variant
+    # evaluation at 256 px: the full grid (the arbiter) once, then each serving variant
     full = full_grid(256, 6)
     fe, me, gte = config4_batch_cached(seed + 10 ** 7, n_eval, dev, scene)
     ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cached = None
-    if judge and os.path.exists(judge):
-        z = np.load(judge)
+    if full_grid_cache and os.path.exists(full_grid_cache):
+        z = np.load(full_grid_cache)
         if int(z["n_eval"]) == n_eval and int(z["seed"]) == seed and bool(z.get("scene", False)) == scene:
             cached = z
     if cached is not None:
@@ -539,8 +539,8 @@ def experiment(n_train: int, n_eval: int, epochs: int, seed: int, out_dir: str, 
         ev[1].record()
         torch.cuda.synchronize()
         t_full = ev[0].elapsed_time(ev[1]) / 1e3
-        if judge:
-            np.savez(judge, truth=truth, cost=tcost, n_eval=n_eval, seed=seed, scene=scene)
+        if full_grid_cache:
+            np.savez(full_grid_cache, truth=truth, cost=tcost, n_eval=n_eval, seed=seed, scene=scene)
     # how often the label resolution's argmin is the evaluation resolution's
     lab_e, _ = grid_argmins(downsample(fe, 256 // label_side), downsample(me, 256 // label_side), full_l)
     same = np.all(np.isclose(to_units(lab_e, lo_l, hi_l), to_units(truth, full.matrix()[0], full.matrix()[1]),
@@ -664,8 +664,9 @@ if __name__ == "__main__":
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--scene", action="store_true",
                     help="moving images see the fixed image's mirror continuation past its edges (no black borders)")
-    ap.add_argument("--judge", default=None, help=".npz of the full grid's argmins of the held-out pairs (reused "
-                                                  "when it matches --eval and --seed, else written)")
+    ap.add_argument("--full-grid-cache", default=None,
+                    help=".npz of the full grid's argmins of the held-out pairs (reused when it matches --eval "
+                         "and --seed, else written)")
     ap.add_argument("--net-timing", action="store_true",
                     help="only time the network's forward pass and training step on random pairs")
     a = ap.parse_args()
@@ -678,5 +679,5 @@ if __name__ == "__main__":
         vs = [tuple(int(x) for x in v) for v in vs]
     print(json.dumps(experiment(a.train, a.eval, a.epochs, a.seed, a.out, label_side=a.label_side,
                                 min_values=a.min_values, max_values=a.max_values, checkpoint=a.checkpoint,
-                                variants=vs, init=a.init, labels=a.labels, lr=a.lr, judge=a.judge,
-                                mode=a.mode, scene=a.scene)))
+                                variants=vs, init=a.init, labels=a.labels, lr=a.lr,
+                                full_grid_cache=a.full_grid_cache, mode=a.mode, scene=a.scene)))
