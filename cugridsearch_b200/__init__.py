@@ -103,10 +103,16 @@ class CudaGrid:
 
     @classmethod
     def from_ranges(cls, start, end, count) -> "CudaGrid":
+        """setStartPoint, setEndPoint, setNumSamples.  Each setter's update recomputes every axis
+        from its start, end and count alone, and the counts are set last, so one update after
+        all three rows leaves the same grid as the three updates."""
         g = cls(len(start))
-        g.setStartPoint(start)
-        g.setEndPoint(end)
-        g.setNumSamples(count)
+        for row, vals in ((g.g.start, start), (g.g.end, end), (g.g.count, count)):
+            if len(vals) != g.g.dims:
+                raise ValueError(f"expected {g.g.dims} values")
+            for a, v in enumerate(vals):
+                row[a] = float(np.float32(v))
+        g.update()
         return g
 
     def getDimension(self) -> int:

@@ -188,15 +188,21 @@ def _batch_search(cost, fixed, moving, grids, device, dump=None):
     valid (n,), points evaluated).  dump: indices of the pairs whose whole cost arrays are
     wanted; they are then returned as a fifth element (dict index -> numpy array)."""
     import torch
-    from . import Batch, BatchPair, CudaImage, read_result, result_buffer
-    res = [result_buffer(device) for _ in grids]
+    from . import Batch, BatchPair, CudaImage, read_result
+    # the results in one device block (one copy back), pair i's at bytes [i st, i st + rb), each
+    # slot 128-byte aligned as a result buffer of its own would be
+    rb = C.sizeof(_abi.CgsArgmin)
+    st = (rb + 127) // 128 * 128
+    block = torch.empty(len(grids) * st, dtype=torch.uint8, device=device)
+    res = [block[i * st:i * st + rb] for i in range(len(grids))]
     dumps = {i: torch.empty(grids[i].numElements(), dtype=torch.float32, device=device) for i in (dump or ())}
     pairs = [BatchPair(cost, CudaImage(moving[i]), CudaImage(fixed[i]), g, res[i], dumps.get(i))
              for i, g in enumerate(grids)]
     with Batch(pairs) as b:
         b.launch()
         torch.cuda.synchronize(device)
-    out = [read_result(r) for r in res]
+    host = block.cpu()
+    out = [read_result(host[i * st:i * st + rb]) for i in range(len(grids))]
     params = np.stack([o.params for o in out]).astype(np.float64)
     costs = np.array([o.cost for o in out], np.float64)
     valid = np.array([o.valid and o.status == 0 for o in out])

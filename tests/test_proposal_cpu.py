@@ -241,3 +241,44 @@ def test_refine_serve_logic_with_oracle_search(lib, monkeypatch):
     np.testing.assert_allclose(r2.costs[fb], tcost[fb], rtol=1e-6, atol=1e-7)
     assert calls[-1] == int(fb.sum())  # the fallback searches the full grid of those pairs only
     assert np.all(r2.params >= lo - 1e-6) and np.all(r2.params <= hi + 1e-6)
+
+
+def test_batch_search_reads_every_pair_result(lib, monkeypatch):
+    """_batch_search hands each pair a slot of one result block and reads all of them with one
+    copy: a stand-in batch writes a distinct result through each pair's result pointer, and each
+    comes back to its own pair."""
+    import ctypes as C
+    import cugridsearch_b200 as cgs
+    from cugridsearch_b200 import _abi
+    from cugridsearch_b200 import proposal as P
+
+    class FakeBatch:
+        def __init__(self, pairs, plan=None):
+            self.pairs = pairs
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *a):
+            return False
+
+        def launch(self, stream=None):
+            for i, bp in enumerate(self.pairs):
+                r = _abi.CgsArgmin()
+                r.cost, r.valid, r.index = -0.5 - i, 1, 1000 + i
+                for a in range(8):
+                    r.params[a] = float(i + a)
+                addr = bp.result.data_ptr()
+                assert addr % 8 == 0
+                C.memmove(addr, C.addressof(r), C.sizeof(r))
+
+    monkeypatch.setattr(cgs, "Batch", FakeBatch)
+    monkeypatch.setattr(cgs, "CudaImage", lambda t: t)  # host tensors stand in for the images
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    full = P.full_grid(256, 6)
+    n = 5
+    img = torch.zeros((n, 4, 4))
+    params, costs, valid, pts = P._batch_search("ZNCC", img, img, [full] * n, torch.device("cpu"))
+    assert valid.all() and pts == n * full.numElements()
+    np.testing.assert_array_equal(costs, -0.5 - np.arange(n))
+    np.testing.assert_array_equal(params, np.arange(n)[:, None] + np.arange(8)[None, :])
