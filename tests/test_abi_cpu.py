@@ -59,6 +59,23 @@ def test_grid_arithmetic_matches_reference(lib, start, end, count):
         np.testing.assert_array_equal(g.getGridPoint(int(idx)), O.grid_point(og, int(idx))[: len(start)])
 
 
+def test_from_ranges_equals_the_setter_sequence(lib):
+    """from_ranges sets the three rows and updates once; the reference's setter sequence (start,
+    end, counts, each followed by an update) leaves the same grid, collapsed axes included."""
+    import cugridsearch_b200 as cgs
+    rng = np.random.default_rng(3)
+    for _ in range(2000):
+        s = rng.uniform(-50, 50, 8)
+        e = s + np.where(rng.random(8) < 0.25, rng.choice([0.0, 1e-9, 1e-6, 1e-4], 8), rng.uniform(-10, 30, 8))
+        c = rng.integers(1, 9, 8).astype(float)
+        a = cgs.CudaGrid.from_ranges(list(s), list(e), list(c))
+        b = cgs.CudaGrid(8)
+        b.setStartPoint(list(s))
+        b.setEndPoint(list(e))
+        b.setNumSamples(list(c))
+        assert bytes(a.g) == bytes(b.g)
+
+
 def test_collapsed_axis(lib):
     import cugridsearch_b200 as cgs
     g = cgs.CudaGrid.from_ranges([0.0, 1.0], [0.0, 2.0], [10, 3])  # start == end collapses to 1 sample
