@@ -374,36 +374,38 @@ def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", valu
     probe_cost = np.where(v[n:], c[n:], np.inf)
     left_levels = np.full(n, levels)
     left_walks = np.full(n, walks)
+
+    def grid_rows(gs):
+        # each grid's start, resolution and sample counts as the library computed them
+        return (np.array([g.g.start[:d] for g in gs], np.float64), np.array([g.g.resolution[:d] for g in gs],
+                                                                              np.float64),
+                np.array([g.g.count[:d] for g in gs], np.float64).astype(np.int64))
+
     active = np.arange(n)
-    cur_p, cur_c, cur_v, cur_g = p[:n], c[:n], v[:n], grids
+    cur_p, cur_c, cur_v = p[:n], c[:n], v[:n]
+    ga, gr, gc = grid_rows(grids)
+    span = hi - lo
     while True:
-        nxt, ngrids = [], []
-        for j, i in enumerate(active):
-            if cur_v[j] and cur_c[j] < costs[i]:
-                params[i], costs[i] = cur_p[j], cur_c[j]
-            if not cur_v[j] or not np.isfinite(costs[i]):
-                continue
-            g = cur_g[j]
-            a = np.array([g.g.start[k] for k in range(d)], np.float64)
-            r = np.array([g.g.resolution[k] for k in range(d)], np.float64)
-            cnt = np.array([int(g.g.count[k]) for k in range(d)])
-            loc = np.where(cnt > 1, np.rint((params[i] - a) / np.where(r != 0, r, 1.0)), 0).astype(np.int64)
-            edge = ((loc == 0) & (a > lo + 1e-9 * (hi - lo))) | \
-                   ((loc == cnt - 1) & (a + r * (cnt - 1) < hi - 1e-9 * (hi - lo)))
-            if edge.any() and left_walks[i] > 0:
-                left_walks[i] -= 1
-            elif left_levels[i] > 0:
-                left_levels[i] -= 1
-                half[i] = half[i] / 2.0
-            else:
-                continue
-            nxt.append(i)
-            ngrids.append(local(params[i], half[i]))
-        if not nxt:
+        # every active pair at once: keep its best point, then walk (best point on an inner
+        # edge of its local grid), halve (levels left) or stop
+        better = cur_v & (cur_c < costs[active])
+        params[active[better]] = cur_p[better]
+        costs[active[better]] = cur_c[better]
+        alive = cur_v & np.isfinite(costs[active])
+        loc = np.where(gc > 1, np.rint((params[active] - ga) / np.where(gr != 0, gr, 1.0)), 0).astype(np.int64)
+        edge = ((loc == 0) & (ga > lo + 1e-9 * span)) | ((loc == gc - 1) & (ga + gr * (gc - 1) < hi - 1e-9 * span))
+        walk = alive & edge.any(axis=1) & (left_walks[active] > 0)
+        halve = alive & ~walk & (left_levels[active] > 0)
+        left_walks[active[walk]] -= 1
+        left_levels[active[halve]] -= 1
+        half[active[halve]] = half[active[halve]] / 2.0
+        nxt = active[walk | halve]
+        if not nxt.size:
             break
-        active = np.array(nxt)
+        ngrids = [local(params[i], half[i]) for i in nxt]
+        active = nxt
         cur_p, cur_c, cur_v, k = _batch_search(cost, fixed[active], moving[active], ngrids, fixed.device)
-        cur_g = ngrids
+        ga, gr, gc = grid_rows(ngrids)
         pts += k
         d2h += len(ngrids) * rbytes
     fallback = ~(costs <= probe_cost)
