@@ -107,11 +107,11 @@ class CudaGrid:
         from its start, end and count alone, and the counts are set last, so one update after
         all three rows leaves the same grid as the three updates."""
         g = cls(len(start))
+        d = g.g.dims
         for row, vals in ((g.g.start, start), (g.g.end, end), (g.g.count, count)):
-            if len(vals) != g.g.dims:
-                raise ValueError(f"expected {g.g.dims} values")
-            for a, v in enumerate(vals):
-                row[a] = float(np.float32(v))
+            if len(vals) != d:
+                raise ValueError(f"expected {d} values")
+            row[:d] = np.asarray(vals, np.float64).astype(np.float32).tolist()  # rounded to FP32 as the setters do
         g.update()
         return g
 

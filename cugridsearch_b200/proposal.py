@@ -360,8 +360,7 @@ def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", valu
 
     def local(c, h):
         a, b = np.maximum(lo, c - h), np.minimum(hi, c + h)
-        cnt = [float(values) if b[k] > a[k] else 1.0 for k in range(d)]
-        return CudaGrid.from_ranges([float(v) for v in a], [float(v) for v in np.where(b > a, b, a)], cnt)
+        return CudaGrid.from_ranges(a, np.where(b > a, b, a), np.where(b > a, float(values), 1.0))
 
     probe = coarse_grid(full, probe_values)
     params = np.zeros((n, d))
