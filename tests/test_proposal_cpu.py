@@ -282,3 +282,110 @@ def test_batch_search_reads_every_pair_result(lib, monkeypatch):
     assert valid.all() and pts == n * full.numElements()
     np.testing.assert_array_equal(costs, -0.5 - np.arange(n))
     np.testing.assert_array_equal(params, np.arange(n)[:, None] + np.arange(8)[None, :])
+
+
+def _refine_per_pair(net, n, full, search, values, levels, spread, min_half, walks):
+    """The refinement serving's rules applied pair by pair (a restatement for the test): keep the
+    best point, walk on an inner edge while walks are left, else halve while levels are left."""
+    from cugridsearch_b200 import CudaGrid
+    from cugridsearch_b200 import proposal as P
+    d = 8
+    lo, hi = full.matrix()[0].astype(np.float64), full.matrix()[1].astype(np.float64)
+    out = net.forward(None, None).numpy().astype(np.float64)
+    centre = P.from_units(np.clip(out[:, :d], -1, 1), lo, hi)
+    half = np.clip(spread * np.exp(np.clip(out[:, 8:], -12, 4)), min_half, 1.0) * (hi - lo) / 2
+
+    def local(c, h):
+        a, b = np.maximum(lo, c - h), np.minimum(hi, c + h)
+        return CudaGrid.from_ranges(list(a), list(np.where(b > a, b, a)),
+                                    [values if b[k] > a[k] else 1 for k in range(d)])
+
+    probe = P.coarse_grid(full, 3)
+    grids = [local(centre[i], half[i]) for i in range(n)]
+    p, c, v, pts = search(grids + [probe] * n)
+    probe_cost = np.where(v[n:], c[n:], np.inf)
+    params, costs = np.zeros((n, d)), np.full(n, np.inf)
+    lev, wal = [levels] * n, [walks] * n
+    active, cur = list(range(n)), (p[:n], c[:n], v[:n], grids)
+    while True:
+        nxt, ng = [], []
+        for j, i in enumerate(active):
+            cp, cc, cv, cg = cur[0][j], cur[1][j], cur[2][j], cur[3][j]
+            if cv and cc < costs[i]:
+                params[i], costs[i] = cp, cc
+            if not cv or not np.isfinite(costs[i]):
+                continue
+            a = np.array(cg.g.start[:d], np.float64)
+            r = np.array(cg.g.resolution[:d], np.float64)
+            cnt = np.array(cg.g.count[:d]).astype(int)
+            loc = np.where(cnt > 1, np.rint((params[i] - a) / np.where(r != 0, r, 1.0)), 0)
+            edge = ((loc == 0) & (a > lo + 1e-9 * (hi - lo))) | \
+                ((loc == cnt - 1) & (a + r * (cnt - 1) < hi - 1e-9 * (hi - lo)))
+            if edge.any() and wal[i] > 0:
+                wal[i] -= 1
+            elif lev[i] > 0:
+                lev[i] -= 1
+                half[i] = half[i] / 2
+            else:
+                continue
+            nxt.append(i)
+            ng.append(local(params[i], half[i]))
+        if not nxt:
+            break
+        p2, c2, v2, k = search(ng)
+        pts += k
+        active, cur = nxt, (p2, c2, v2, ng)
+    fb = ~(costs <= probe_cost)
+    if fb.any():
+        pf, cf, _, k = search([full] * int(fb.sum()))
+        pts += k
+        params[fb], costs[fb] = pf, cf
+    return params, costs, fb, pts
+
+
+def test_refine_serve_decisions_match_the_per_pair_rules(lib, monkeypatch):
+    """refine_serve takes its keep / walk / halve / stop decisions for all active pairs at once;
+    on stand-in searches (deterministic in the grid, some results invalid) its answers, fallbacks
+    and point counts equal the rules applied pair by pair."""
+    from cugridsearch_b200 import proposal as P
+    full = P.full_grid(256, 6)
+    lo, hi = full.matrix()[0].astype(np.float64), full.matrix()[1].astype(np.float64)
+
+    def stand_in(seed):
+        tgt = lo + (hi - lo) * np.random.default_rng(seed).uniform(0.1, 0.9, 8)
+
+        def search(grids):
+            ps, cs, vs = [], [], []
+            for g in grids:
+                key = int(abs(np.sum(np.array(g.g.start[:8]) * 1.37 + np.array(g.g.end[:8]))) * 1e6) % (2 ** 32)
+                rs = np.random.default_rng([seed, key])
+                q = np.array(g.getGridPoint(int(rs.integers(0, g.numElements()))), np.float64)
+                ps.append(q)
+                cs.append(float(np.sum(((q - tgt) / (hi - lo)) ** 2)) + rs.uniform(0, 1e-3))
+                vs.append(rs.random() > 0.05)
+            return np.stack(ps), np.array(cs), np.array(vs), sum(g.numElements() for g in grids)
+        return search
+
+    class Net:
+        def __init__(self, seed, n):
+            r = np.random.default_rng(seed)
+            self.out = np.concatenate([r.uniform(-1, 1, (n, 8)), r.uniform(-6, 1, (n, 8))], 1).astype(np.float32)
+
+        def forward(self, f, m):
+            return torch.from_numpy(self.out)
+
+    fallbacks = 0
+    for seed in range(24):
+        n = 1 + seed % 7
+        kw = dict(values=3, levels=1 + seed % 4, spread=2.0, min_half=0.02, walks=seed % 3)
+        search = stand_in(seed)
+        monkeypatch.setattr(P, "_batch_search", lambda cost, f, m, grids, dev, dump=None: search(grids))
+        img = torch.zeros((n, 4, 4))
+        r = P.refine_serve(Net(seed, n), img, img, full, **kw)
+        p, c, fb, pts = _refine_per_pair(Net(seed, n), n, full, search, **kw)
+        np.testing.assert_array_equal(r.params, p)
+        np.testing.assert_array_equal(r.costs, c)
+        np.testing.assert_array_equal(r.fallback, fb)
+        assert r.points == pts
+        fallbacks += int(fb.sum())
+    assert fallbacks > 0  # the stand-in exercises the fallback too
