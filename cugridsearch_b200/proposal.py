@@ -376,9 +376,10 @@ def refine_serve(net: ProposalNet, fixed, moving, full, cost: str = "ZNCC", valu
 
     def grid_rows(gs):
         # each grid's start, resolution and sample counts as the library computed them
-        return (np.array([g.g.start[:d] for g in gs], np.float64), np.array([g.g.resolution[:d] for g in gs],
-                                                                              np.float64),
-                np.array([g.g.count[:d] for g in gs], np.float64).astype(np.int64))
+        starts = np.array([g.g.start[:d] for g in gs], np.float64)
+        steps = np.array([g.g.resolution[:d] for g in gs], np.float64)
+        counts = np.array([g.g.count[:d] for g in gs], np.float64).astype(np.int64)
+        return starts, steps, counts
 
     active = np.arange(n)
     cur_p, cur_c, cur_v = p[:n], c[:n], v[:n]
