@@ -224,17 +224,19 @@ static cgs_status enqueue_launch(const cgs_batch &b, cudaStream_t s) {
     const PrepParams *qs = b.d_prep;
     void *pargs[] = {&qs};
     CGS_CUDA(cudaLaunchKernel(batch_prep_kernel_fn(), dim3(px, b.n), dim3(256), pargs, 0, s), "batch_prep_kernel");
-    if (b.g_n > 0) CGS_CUDA(launch_span_prep_batch(b.d_gprep, (int)b.g_n, b.g_prep_blocks, s), "span_prep_batch_kernel");
+    // the multi-pair span kernel first: its pairs take the least time each, so running them
+    // before the per-sample pairs lowers the pairs' completion times (the launch takes as long)
+    if (b.g_n > 0) {
+        CGS_CUDA(launch_span_prep_batch(b.d_gprep, (int)b.g_n, b.g_prep_blocks, s), "span_prep_batch_kernel");
+        SpanBatchParams ga = b.g_args;
+        void *gargs[] = {&ga};
+        CGS_CUDA(cudaLaunchKernel(b.g_kfn, dim3(b.g_blocks), dim3(16 * 32), gargs, b.g_smem, s), "span_batch_kernel");
+    }
     BatchParams a = batch_args(b, false, b.total_tasks);
     void *kargs[] = {&a};
     if (b.total_tasks > 0)
         CGS_CUDA(cudaLaunchKernel(b.kfn, dim3(b.blocks), dim3(b.plan.warps_per_block * 32), kargs, b.smem, s),
                  "batch_kernel");
-    if (b.g_n > 0) {
-        SpanBatchParams ga = b.g_args;
-        void *gargs[] = {&ga};
-        CGS_CUDA(cudaLaunchKernel(b.g_kfn, dim3(b.g_blocks), dim3(16 * 32), gargs, b.g_smem, s), "span_batch_kernel");
-    }
     for (uint32_t j = 0; j < b.n; j++) {
         if (b.route[j] != 2) continue;
         stamp_kernel<<<1, 1, 0, s>>>(b.t_start + j);
