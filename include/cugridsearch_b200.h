@@ -275,8 +275,9 @@ cgs_status cgs_quantize_image(cgs_image *img, float mod, cgs_stream_t stream);
 
 /* ---------------------------------------------------------------- batched search
  *
- * Many image pairs of uneven sizes, each with its own grid and cost, evaluated by ONE
- * persistent sm_100a launch.  The reference searches one pair per call and its callers loop
+ * Many image pairs of uneven sizes, each with its own grid and cost, evaluated by one recorded
+ * launch sequence (a persistent kernel over the per-sample pairs, one multi-pair span kernel over
+ * the ZNCC pairs).  The reference searches one pair per call and its callers loop
  * over pairs and refinement levels (src/gpu/cudaGridSearch_main_mi.cu:312-363, one
  * search_by_value + find_extrema per pass); a batch replaces that loop.  Each pair's costs and
  * argmin equal those of cgs_search on the same pair: bit for bit with block_split = 0, within
@@ -317,15 +318,17 @@ typedef struct cgs_tune_entry {
 
 typedef struct cgs_batch cgs_batch; /* opaque handle */
 
-/* Creates a batch: validates every pair, lays out device scratch for all of them (one
- * allocation, held until cgs_batch_destroy), orders the pairs by estimated work (cheapest
- * first) and records one CUDA graph -- clear scratch, stage every pair, the persistent batch
- * kernel over the pairs' tasks, then, pair after pair, the launches of cgs_search for the ZNCC
- * and MI pairs that cgs_search runs on its span kernels (fast sampling, no per-sample flag;
- * their results are cgs_search's bit for bit, FP64 verification included) -- for the plan
- * (NULL: 4 points per warp, 16 warps, warp-private histograms; 2 points per warp, then
- * block-shared histograms, where those do not fit).  The images, dumps and results are bound to the
- * handle: update image CONTENTS in place between launches.  Errors name the failing pair. */
+/* Creates a batch: validates every pair, lays out device scratch for all of them (one block
+ * from the library's pool, held until cgs_batch_destroy), orders the pairs by estimated work
+ * (cheapest first) and records one CUDA graph: clear scratch, stage every pair; the ZNCC pairs
+ * that cgs_search runs on its span kernel (fast sampling, no per-sample flag) in one multi-pair
+ * span launch, with cgs_search's costs and argmins bit for bit; the other pairs in the
+ * persistent batch kernel, for the plan (NULL: 4 points per warp, 16 warps, warp-private
+ * histograms; 2 points per warp, then block-shared histograms, where those do not fit); then,
+ * pair after pair, cgs_search's own launches for MI pairs that it runs on its MI span kernel and
+ * whose grids have at least 4 span tasks per SM (their results are cgs_search's, FP64
+ * verification included).  The images, dumps and results are bound to the handle: update image
+ * CONTENTS in place between launches.  Errors name the failing pair. */
 cgs_status cgs_batch_create(const cgs_pair *pairs, int32_t n, const cgs_batch_plan *plan, cgs_batch **batch);
 
 /* Replays the batch graph on `stream` (asynchronous).  Launches of one batch are serialised. */
