@@ -149,6 +149,11 @@ def test_batch_arguments_fail_before_device_work(lib):
     bad_bins = abi.CgsOptions(abi.COSTS["MI"], 48, 0.0, 0, 0, 0)
     assert L.cgs_batch_create(pairs(abi.CgsPair(img, img, g, bad_bins, None, 64)), 1, None, C.byref(h)) == 1
     assert not h.value
+    # the handle's queries refuse a null handle or output
+    k = C.c_int32(-1)
+    assert L.cgs_batch_kernel_launches(None, C.byref(k)) == 1 and k.value == -1
+    t = (C.c_uint64 * 1)()
+    assert L.cgs_batch_pair_times(None, t, t) == 1
 
 
 def test_batch_struct_layout():
